@@ -1,0 +1,395 @@
+"""CPU oracle for the DF-RHF energy and analytic forces.
+
+TEST INFRASTRUCTURE ONLY.  Tests, ``__graft_entry__.smoke()`` and the CPU
+baseline leg of ``bench.py`` use it as the checker; no product path imports it.
+
+This is a plain restatement of the reference's CPU density-fitting RHF path:
+
+* integrals from ``liboracle.so`` (``df_oracle.c``; McMurchie-Davidson);
+* metric factor with the relative eigenvalue cutoff
+  (reference ``src/integrals/density_fitting_metric.cpp:101-154``);
+* whitened three-centre tensor B = A M^{-1/2}
+  (``src/scf/density_fitting.cpp:711-764``);
+* RI-J and density-form RI-K (``src/scf/density_fitting.cpp:101-222``);
+* the SCF loop: core guess, F = H + J - K/2, Pulay DIIS on FDS - SDF,
+  convergence on |dE|, rms(dD) and max|FDS - SDF|
+  (``src/scf/solver/mean_field_driver.cpp:233``,
+  ``src/scf/cuda/scf_convergence_policy.cuh:28-37``);
+* reverse weights Abar and Mbar+ (``src/scf/density_fitting.cpp:464-594``),
+  the spectral metric response (``density_fitting_metric.cpp:50-99``) and the
+  weighted derivative contractions (``src/integrals/s_integrals.cpp:1073,2187``);
+* forces F = -(g_1e + g_DF + dV_nn) (``src/scf/rhf.cpp:856-868``).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+import subprocess
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+from vibeqc_b200 import basis as bas
+
+HERE = Path(__file__).resolve().parent
+_LIB_PATH = HERE / "liboracle.so"
+NSMAX, NCMAX, LMAX = 13, 28, 6
+
+
+def build() -> Path:
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return _LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not _LIB_PATH.exists():
+            build()
+        _lib = ctypes.CDLL(str(_LIB_PATH))
+        for name in ("oracle_int3c", "oracle_int2c", "oracle_int1e", "oracle_grad3c",
+                     "oracle_grad2c", "oracle_grad1e", "oracle_boys"):
+            getattr(_lib, name).restype = None
+    return _lib
+
+
+class _CBasis(ctypes.Structure):
+    _fields_ = [
+        ("nshell", ctypes.c_int),
+        ("l", ctypes.c_void_p),
+        ("atom", ctypes.c_void_p),
+        ("nprim", ctypes.c_void_p),
+        ("prim_off", ctypes.c_void_p),
+        ("func_off", ctypes.c_void_p),
+        ("exps", ctypes.c_void_p),
+        ("coefs", ctypes.c_void_p),
+        ("nfunc", ctypes.c_int),
+        ("trans", ctypes.c_void_p),
+        ("nout", ctypes.c_void_p),
+    ]
+
+
+class OracleBasis:
+    """Shell arrays in the layout the C oracle reads; functions in shell order."""
+
+    def __init__(self, shells, spherical: bool = True):
+        self.shells = list(shells)
+        self.spherical = spherical
+        ls, atoms, nprim, poff, foff, exps, coefs = [], [], [], [], [], [], []
+        f = p = 0
+        for s in self.shells:
+            a, c = bas.normalized_coefficients(s)
+            ls.append(s.angular_momentum)
+            atoms.append(s.atom_index)
+            nprim.append(len(a))
+            poff.append(p)
+            foff.append(f)
+            exps.extend(a)
+            coefs.extend(c)
+            p += len(a)
+            f += bas.nfunc(s.angular_momentum, spherical)
+        if max(ls) + 1 > LMAX:
+            raise ValueError("oracle supports l <= 5")
+        self.nfunc = f
+        i32 = lambda v: np.ascontiguousarray(v, dtype=np.int32)  # noqa: E731
+        self._l, self._atom, self._nprim = i32(ls), i32(atoms), i32(nprim)
+        self._poff, self._foff = i32(poff), i32(foff)
+        self._exps = np.ascontiguousarray(exps, dtype=np.float64)
+        self._coefs = np.ascontiguousarray(coefs, dtype=np.float64)
+        trans = np.zeros((LMAX + 1, NSMAX, NCMAX))
+        nout = np.zeros(LMAX + 1, dtype=np.int32)
+        for l in range(LMAX + 1):
+            t = bas.transform_matrix(l, spherical) if 2 * l + 1 <= NSMAX or not spherical else None
+            if t is None or t.shape[0] > NSMAX:
+                continue
+            trans[l, : t.shape[0], : t.shape[1]] = t
+            nout[l] = t.shape[0]
+        self._trans, self._nout = trans, nout
+        self.c = _CBasis(
+            len(ls),
+            self._l.ctypes.data,
+            self._atom.ctypes.data,
+            self._nprim.ctypes.data,
+            self._poff.ctypes.data,
+            self._foff.ctypes.data,
+            self._exps.ctypes.data,
+            self._coefs.ctypes.data,
+            f,
+            self._trans.ctypes.data,
+            self._nout.ctypes.data,
+        )
+
+
+def _ptr(a: np.ndarray):
+    assert a.flags.c_contiguous
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def boys(mmax: int, t: float) -> np.ndarray:
+    out = np.zeros(mmax + 1)
+    lib().oracle_boys(ctypes.c_int(mmax), ctypes.c_double(t), _ptr(out))
+    return out
+
+
+def int3c(orb: OracleBasis, aux: OracleBasis, xyz: np.ndarray) -> np.ndarray:
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+    out = np.zeros((orb.nfunc, orb.nfunc, aux.nfunc))
+    lib().oracle_int3c(ctypes.byref(orb.c), ctypes.byref(aux.c), _ptr(xyz), _ptr(out))
+    return out
+
+
+def int2c(aux: OracleBasis, xyz: np.ndarray) -> np.ndarray:
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+    out = np.zeros((aux.nfunc, aux.nfunc))
+    lib().oracle_int2c(ctypes.byref(aux.c), _ptr(xyz), _ptr(out))
+    return out
+
+
+def int1e(orb: OracleBasis, xyz: np.ndarray, charges: np.ndarray):
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+    z = np.ascontiguousarray(charges, dtype=np.float64)
+    n = orb.nfunc
+    s, t, v = np.zeros((n, n)), np.zeros((n, n)), np.zeros((n, n))
+    lib().oracle_int1e(ctypes.byref(orb.c), ctypes.c_int(len(z)), _ptr(xyz), _ptr(z),
+                       _ptr(s), _ptr(t), _ptr(v))
+    return s, t, v
+
+
+def grad3c(orb, aux, xyz, abar) -> np.ndarray:
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+    abar = np.ascontiguousarray(abar, dtype=np.float64)
+    g = np.zeros(xyz.size)
+    lib().oracle_grad3c(ctypes.byref(orb.c), ctypes.byref(aux.c), ctypes.c_int(len(xyz)),
+                        _ptr(xyz), _ptr(abar), _ptr(g))
+    return g.reshape(-1, 3)
+
+
+def grad2c(aux, xyz, mbar) -> np.ndarray:
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+    mbar = np.ascontiguousarray(mbar, dtype=np.float64)
+    g = np.zeros(xyz.size)
+    lib().oracle_grad2c(ctypes.byref(aux.c), ctypes.c_int(len(xyz)), _ptr(xyz), _ptr(mbar),
+                        _ptr(g))
+    return g.reshape(-1, 3)
+
+
+def grad1e(orb, xyz, charges, dens, wdens) -> np.ndarray:
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+    z = np.ascontiguousarray(charges, dtype=np.float64)
+    g = np.zeros(xyz.size)
+    lib().oracle_grad1e(ctypes.byref(orb.c), ctypes.c_int(len(z)), _ptr(xyz), _ptr(z),
+                        _ptr(np.ascontiguousarray(dens)), _ptr(np.ascontiguousarray(wdens)),
+                        _ptr(g))
+    return g.reshape(-1, 3)
+
+
+def nuclear_repulsion(xyz: np.ndarray, charges: np.ndarray) -> tuple[float, np.ndarray]:
+    e = 0.0
+    g = np.zeros_like(xyz)
+    for i in range(len(xyz)):
+        for j in range(i):
+            d = xyz[i] - xyz[j]
+            r = math.sqrt(d @ d)
+            e += charges[i] * charges[j] / r
+            f = -charges[i] * charges[j] / r**3 * d
+            g[i] += f
+            g[j] -= f
+    return e, g
+
+
+# --------------------------------------------------------------------------
+# metric factor and its spectral response
+# --------------------------------------------------------------------------
+
+@dataclass
+class MetricFactor:
+    eigenvalues: np.ndarray
+    eigenvectors: np.ndarray
+    keep: np.ndarray
+    inv_sqrt: np.ndarray
+    pinv: np.ndarray
+    rank: int
+    condition: float
+
+
+def factor_metric(m: np.ndarray, relative_threshold: float = 1e-10) -> MetricFactor:
+    """Eigen-based M^{-1/2} dropping lambda <= rel * lambda_max.
+
+    Reference: ``src/integrals/density_fitting_metric.cpp:101-154``.
+    """
+    if not np.all(np.isfinite(m)):
+        raise FloatingPointError("non-finite metric")
+    lam, v = np.linalg.eigh(0.5 * (m + m.T))
+    lmax = lam[-1]
+    if not lmax > 0:
+        raise FloatingPointError("metric has no positive eigenvalue")
+    keep = lam > relative_threshold * lmax
+    vk = v[:, keep]
+    inv_sqrt = (vk / np.sqrt(lam[keep])) @ vk.T
+    pinv = (vk / lam[keep]) @ vk.T
+    return MetricFactor(lam, v, keep, inv_sqrt, pinv, int(keep.sum()),
+                        float(lmax / lam[keep][0]))
+
+
+def metric_response(f: MetricFactor, mbar_plus: np.ndarray, relative_threshold=1e-10) -> np.ndarray:
+    """Adjoint of M -> pinv(M) through the thresholded spectral map.
+
+    Divided differences (f(li) - f(lj)) / (li - lj) with f = 1/l on the retained
+    space and 0 on the discarded one; f'(l) = -1/l^2 on retained diagonal
+    entries.  Reference ``density_fitting_metric.cpp:50-99`` and
+    ``src/tensor/symmetric_matrix_function.cpp:62``.  Eigenvalues within
+    128 eps lambda_max of the cutoff are a rank crossing and rejected.
+    """
+    lam = f.eigenvalues
+    lmax = lam[-1]
+    cut = relative_threshold * lmax
+    if np.any(np.abs(lam - cut) <= 128 * np.finfo(float).eps * lmax):
+        raise FloatingPointError("metric eigenvalue at the rank cutoff")
+    fl = np.where(f.keep, 1.0 / np.where(f.keep, lam, 1.0), 0.0)
+    dl = lam[:, None] - lam[None, :]
+    same = np.abs(dl) <= 1e-14 * lmax
+    with np.errstate(divide="ignore", invalid="ignore"):
+        gam = (fl[:, None] - fl[None, :]) / np.where(same, 1.0, dl)
+    deriv = np.where(f.keep, -fl * fl, 0.0)
+    gam = np.where(same, 0.5 * (deriv[:, None] + deriv[None, :]), gam)
+    v = f.eigenvectors
+    return v @ ((v.T @ mbar_plus @ v) * gam) @ v.T
+
+
+# --------------------------------------------------------------------------
+# DF-RHF
+# --------------------------------------------------------------------------
+
+def molecule_arrays(atoms):
+    z = np.array([bas.atomic_number(s) for s, _ in atoms], dtype=np.float64)
+    xyz = np.array([p for _, p in atoms], dtype=np.float64)
+    return z, xyz
+
+
+@dataclass
+class OracleResult:
+    energy: float
+    forces: np.ndarray | None
+    converged: bool
+    iterations: int
+    density: np.ndarray
+    orbital_energies: np.ndarray
+    coefficients: np.ndarray
+    nocc: int
+    extra: dict
+
+
+def build_jk(b: np.ndarray, d: np.ndarray):
+    """J and density-form K from whitened B (N, N, X)."""
+    rho = np.einsum("mnq,mn->q", b, d, optimize=True)
+    j = b @ rho
+    bq = np.ascontiguousarray(b.transpose(2, 0, 1))
+    k = np.einsum("qml,ls,qsn->mn", bq, d, bq, optimize=True)
+    return j, k
+
+
+def df_rhf(atoms, basis="def2-svp", auxiliary_basis="cc-pvdz-jkfit", *, spherical=True,
+           charge=0, max_iterations=100, energy_tolerance=1e-10, density_tolerance=1e-8,
+           diis_history=8, forces=True, relative_threshold=1e-10) -> OracleResult:
+    z, xyz = molecule_arrays(atoms)
+    orb_sh = bas.expand_shells(z.astype(int), basis)
+    aux_sh = bas.expand_shells(z.astype(int), auxiliary_basis)
+    orb, aux = OracleBasis(orb_sh, spherical), OracleBasis(aux_sh, spherical)
+    nel = int(z.sum()) - charge
+    if nel % 2:
+        raise ValueError("RHF needs an even electron count")
+    nocc = nel // 2
+    s, t, v = int1e(orb, xyz, z)
+    h = t + v
+    m = int2c(aux, xyz)
+    a = int3c(orb, aux, xyz)
+    mf = factor_metric(m, relative_threshold)
+    b = a @ mf.inv_sqrt
+    enuc, gnuc = nuclear_repulsion(xyz, z)
+    sl, sv = np.linalg.eigh(s)
+    xorth = (sv / np.sqrt(sl)) @ sv.T
+
+    def density_from(f):
+        e, cp = np.linalg.eigh(xorth.T @ f @ xorth)
+        c = xorth @ cp
+        return 2.0 * c[:, :nocc] @ c[:, :nocc].T, e, c
+
+    d, eps, coef = density_from(h)
+    e_old = None
+    errs, focks = [], []
+    converged = False
+    it = 0
+    energy = 0.0
+    for it in range(1, max_iterations + 1):
+        j, k = build_jk(b, d)
+        f = h + j - 0.5 * k
+        energy = 0.5 * np.sum(d * (h + f)) + enuc
+        err = f @ d @ s - s @ d @ f
+        err_o = xorth.T @ err @ xorth
+        d_new, eps, coef = None, None, None
+        errs.append(err_o)
+        focks.append(f)
+        errs, focks = errs[-diis_history:], focks[-diis_history:]
+        nh = len(errs)
+        if nh > 1:
+            bm = -np.ones((nh + 1, nh + 1))
+            bm[nh, nh] = 0.0
+            for i in range(nh):
+                for jj in range(nh):
+                    bm[i, jj] = np.sum(errs[i] * errs[jj])
+            rhs = np.zeros(nh + 1)
+            rhs[nh] = -1.0
+            try:
+                w = np.linalg.solve(bm, rhs)[:nh]
+                f_ext = sum(wi * fi for wi, fi in zip(w, focks))
+            except np.linalg.LinAlgError:
+                f_ext = f
+        else:
+            f_ext = f
+        d_new, eps, coef = density_from(f_ext)
+        de = abs(energy - e_old) if e_old is not None else np.inf
+        drms = float(np.sqrt(np.mean((d_new - d) ** 2)))
+        comm = float(np.abs(err).max())
+        e_old = energy
+        if de < energy_tolerance and drms < density_tolerance and comm <= min(1e-8, density_tolerance) * 10:
+            converged = True
+            break
+        d = d_new
+    # final quantities at the density the energy was evaluated with
+    j, k = build_jk(b, d)
+    f = h + j - 0.5 * k
+    energy = 0.5 * np.sum(d * (h + f)) + enuc
+    e_mo, cp = np.linalg.eigh(xorth.T @ f @ xorth)
+    coef = xorth @ cp
+    result = OracleResult(energy, None, converged, it, d, e_mo, coef, nocc, {})
+    if forces:
+        result.forces = -df_rhf_gradient(orb, aux, xyz, z, a, mf, d, coef, e_mo, nocc, gnuc,
+                                         relative_threshold)
+    result.extra.update(nao=orb.nfunc, naux=aux.nfunc, rank=mf.rank, condition=mf.condition)
+    return result
+
+
+def df_rhf_gradient(orb, aux, xyz, z, a, mf, d, coef, e_mo, nocc, gnuc, relative_threshold=1e-10):
+    """Positive energy gradient (natom, 3) at the SCF solution."""
+    cocc = coef[:, :nocc]
+    dmat = 2.0 * cocc @ cocc.T
+    wmat = 2.0 * (cocc * e_mo[:nocc]) @ cocc.T
+    rho = np.einsum("mnp,mn->p", a, dmat, optimize=True)
+    cvec = mf.pinv @ rho
+    aq = np.ascontiguousarray(a.transpose(2, 0, 1))  # (X, N, N)
+    daq = np.einsum("ml,qls,sn->qmn", dmat, aq, dmat, optimize=True)  # D A_Q D
+    abar = dmat[:, :, None] * cvec[None, None, :]
+    abar -= 0.5 * np.einsum("pq,qmn->mnp", mf.pinv, daq, optimize=True)
+    qmat = np.einsum("pmn,qmn->pq", aq, daq, optimize=True)
+    mbar_plus = 0.5 * np.outer(rho, rho) - 0.25 * qmat
+    mbar = metric_response(mf, mbar_plus, relative_threshold)
+    g = grad1e(orb, xyz, z, dmat, wmat)
+    g += grad3c(orb, aux, xyz, abar)
+    g += grad2c(aux, xyz, mbar)
+    g += gnuc
+    return g
