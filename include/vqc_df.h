@@ -1,0 +1,129 @@
+/*
+ * vqc_df.h -- C ABI of the B200 DF-RHF engine (libvqc_b200.so).
+ *
+ * Plain C: device pointers, host pointers, sizes and a cudaStream_t passed as
+ * void*. No C++ or torch types cross this boundary.  Every entry point returns
+ * a status in the reference's generativeqc_status vocabulary
+ * (include/generativeqc/generativeqc.h:23-42 of the reference):
+ *   0 success, 1 invalid argument, 4 not converged, 5 numerical failure,
+ *   6 CUDA error, 7 out of memory.
+ * A thread-local detail string is available from vqc_last_error() (same idea as
+ * generativeqc_context_get_last_detail, generativeqc.h:1231).
+ *
+ * Ownership: the caller owns every input and output buffer; the library
+ * allocates only inside a vqc_plan (device copies of the batch topology), which
+ * vqc_plan_destroy releases (docs/developer/architecture.md:149-153 of the
+ * reference: caller-provided output storage remains caller-owned).
+ * Threading: a plan is not re-entrant; callers serialise use of one plan.
+ */
+#ifndef VQC_DF_H
+#define VQC_DF_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VQC_ABI_VERSION 1u
+
+enum {
+  VQC_STATUS_SUCCESS = 0,
+  VQC_STATUS_INVALID_ARGUMENT = 1,
+  VQC_STATUS_NOT_CONVERGED = 4,
+  VQC_STATUS_NUMERICAL_FAILURE = 5,
+  VQC_STATUS_CUDA_ERROR = 6,
+  VQC_STATUS_OUT_OF_MEMORY = 7
+};
+
+typedef struct vqc_plan vqc_plan;
+
+/*
+ * A ragged batch of molecules with their orbital and auxiliary shells (host
+ * arrays).  Replaces the per-system generativeqc_system_descriptor
+ * (generativeqc.h:586-599: atoms, shells, primitives) plus the auxiliary-basis
+ * system handle (generativeqc.h:733-740), batched the way
+ * generativeqc_batch_prepare (generativeqc.h:1435) receives a list of systems.
+ * Shell atom indices are global (into the concatenated atom list).  Primitive
+ * coefficients already include primitive and contraction normalisation.
+ * Auxiliary shells must be sorted by angular momentum within each molecule.
+ */
+typedef struct {
+  uint32_t struct_size;
+  uint32_t abi_version;
+  int32_t nmol;
+  int32_t spherical;                 /* 1: real spherical, 0: Cartesian */
+  const int32_t* mol_atom_offset;    /* [nmol+1] */
+  const int32_t* mol_shell_offset;   /* [nmol+1] orbital shells */
+  const int32_t* mol_aux_offset;     /* [nmol+1] auxiliary shells */
+  const double* atom_charge;         /* [natom] nuclear charges */
+  const int32_t* shell_l;            /* orbital shells */
+  const int32_t* shell_atom;
+  const int32_t* shell_nprim;
+  const int32_t* shell_prim_off;
+  const double* prim_exp;
+  const double* prim_coef;
+  int32_t nprim;
+  const int32_t* aux_l;              /* auxiliary shells */
+  const int32_t* aux_atom;
+  const int32_t* aux_nprim;
+  const int32_t* aux_prim_off;
+  const double* aux_exp;
+  const double* aux_coef;
+  int32_t naux_prim;
+} vqc_batch_desc;
+
+/* Per-molecule sizes and offsets (elements) into the batch-wide buffers. */
+typedef struct {
+  int32_t nao;        /* orbital functions N */
+  int32_t naux;       /* auxiliary functions X */
+  int32_t natom;
+  int32_t atom_offset;
+  int64_t mat_offset; /* into N*N buffers (S, T, V, D, J, K, F) */
+  int64_t met_offset; /* into X*X buffers (metric) */
+  int64_t a_offset;   /* into packed 3-centre buffers: N(N+1)/2 rows of X */
+} vqc_molecule_info;
+
+const char* vqc_last_error(void);
+uint32_t vqc_abi_version(void);
+
+/* Plan over a batch topology (generativeqc_batch_prepare, generativeqc.h:1435). */
+int vqc_plan_create(const vqc_batch_desc* desc, vqc_plan** out);
+int vqc_plan_destroy(vqc_plan* plan);
+int vqc_plan_totals(const vqc_plan* plan, int64_t* mat_total, int64_t* met_total,
+                    int64_t* a_total, int32_t* natom_total);
+int vqc_plan_molecule(const vqc_plan* plan, int32_t index, vqc_molecule_info* info);
+
+/*
+ * Integrals.  xyz: device [natom][3] Bohr.  Outputs are device buffers sized
+ * by vqc_plan_totals.
+ *   vqc_int1e  -> S, T, V (each mat_total)      reference s_integrals.cpp:1865
+ *   vqc_int2c  -> metric (P|Q) (met_total)      reference s_integrals.cpp:1201
+ *   vqc_int3c  -> A[(mu nu) packed, mu>=nu][P]  reference s_integrals.cpp:1201,
+ *                 df_source_kernels.cu:67 (raw tiles, aux contiguous)
+ */
+int vqc_int1e(vqc_plan* plan, const double* xyz, double* s, double* t, double* v, void* stream);
+int vqc_int2c(vqc_plan* plan, const double* xyz, double* metric, void* stream);
+int vqc_int3c(vqc_plan* plan, const double* xyz, double* a_packed, void* stream);
+
+/*
+ * Gradient contractions (accumulate into grad[natom][3]; the caller zeroes it).
+ *   vqc_grad3c: g += sum Abar[(mu nu) packed][P] d(mu nu|P)/dR, with Abar
+ *               symmetric in (mu, nu) and stored like vqc_int3c's output.
+ *               Replaces generativeqc_system_df_gradient_cuda's 3-centre part
+ *               (generativeqc.h:1312-1333; src/api/c_api_df_gradient.cpp:11).
+ *   vqc_grad2c: g += sum Mbar[P][Q] d(P|Q)/dR (same entry's metric part).
+ *   vqc_grad1e: g += sum D d(T+V)/dR - W dS/dR, nuclear-position terms included
+ *               (reference src/integrals/s_integrals.cpp:2187).
+ */
+int vqc_grad3c(vqc_plan* plan, const double* xyz, const double* abar_packed, double* grad,
+               void* stream);
+int vqc_grad2c(vqc_plan* plan, const double* xyz, const double* mbar, double* grad, void* stream);
+int vqc_grad1e(vqc_plan* plan, const double* xyz, const double* dens, const double* wdens,
+               double* grad, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VQC_DF_H */

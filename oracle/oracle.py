@@ -236,11 +236,13 @@ def factor_metric(m: np.ndarray, relative_threshold: float = 1e-10) -> MetricFac
                         float(lmax / lam[keep][0]))
 
 
-def metric_response(f: MetricFactor, mbar_plus: np.ndarray, relative_threshold=1e-10) -> np.ndarray:
-    """Adjoint of M -> pinv(M) through the thresholded spectral map.
+def metric_response(f: MetricFactor, mbar_plus: np.ndarray, relative_threshold=1e-10,
+                    power: float = -1.0) -> np.ndarray:
+    """Adjoint of M -> f(M) through the thresholded spectral map.
 
-    Divided differences (f(li) - f(lj)) / (li - lj) with f = 1/l on the retained
-    space and 0 on the discarded one; f'(l) = -1/l^2 on retained diagonal
+    f(l) = l**power on the retained space and 0 on the discarded one
+    (power = -1: the pseudoinverse; -1/2: the inverse square root).  Divided
+    differences (f(li) - f(lj)) / (li - lj); f'(l) on retained diagonal
     entries.  Reference ``density_fitting_metric.cpp:50-99`` and
     ``src/tensor/symmetric_matrix_function.cpp:62``.  Eigenvalues within
     128 eps lambda_max of the cutoff are a rank crossing and rejected.
@@ -250,12 +252,13 @@ def metric_response(f: MetricFactor, mbar_plus: np.ndarray, relative_threshold=1
     cut = relative_threshold * lmax
     if np.any(np.abs(lam - cut) <= 128 * np.finfo(float).eps * lmax):
         raise FloatingPointError("metric eigenvalue at the rank cutoff")
-    fl = np.where(f.keep, 1.0 / np.where(f.keep, lam, 1.0), 0.0)
+    safe = np.where(f.keep, lam, 1.0)
+    fl = np.where(f.keep, safe**power, 0.0)
     dl = lam[:, None] - lam[None, :]
     same = np.abs(dl) <= 1e-14 * lmax
     with np.errstate(divide="ignore", invalid="ignore"):
         gam = (fl[:, None] - fl[None, :]) / np.where(same, 1.0, dl)
-    deriv = np.where(f.keep, -fl * fl, 0.0)
+    deriv = np.where(f.keep, power * safe ** (power - 1.0), 0.0)
     gam = np.where(same, 0.5 * (deriv[:, None] + deriv[None, :]), gam)
     v = f.eigenvectors
     return v @ ((v.T @ mbar_plus @ v) * gam) @ v.T

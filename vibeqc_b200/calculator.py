@@ -1,0 +1,309 @@
+"""Drop-in ``Calculator`` / ``PreparedBatch`` for the DF-RHF CUDA path.
+
+Same constructor keywords, methods and result records as the reference's
+``python/generativeqc/calculator.py:157-186`` (``Calculator``), ``:1931``
+(``prepare_batch``), ``:2128`` (``singlepoint``) and
+``python/generativeqc/batch.py:58-121,799`` (``BatchItemResult``,
+``BatchResult``, ``PreparedBatch.execute``).  Units are Bohr and Hartree;
+forces are -dE/dR.  Only ``method="rhf"`` with ``density_fitting="cuda"``
+(or ``"auto"``/``True``) on ``device="cuda"`` is served here; any other
+combination raises ``NotImplementedError`` naming the unsupported option.
+"""
+
+from __future__ import annotations
+
+import threading
+from dataclasses import dataclass, field
+from typing import Iterable, Sequence
+
+import numpy as np
+import torch
+
+from . import _lib
+from .gradient import df_rhf_gradient
+from .plan import make_molecule
+from .scf import Chunk, compute_integrals, run_scf
+
+STATUS_SUCCESS = 0
+STATUS_INVALID_ARGUMENT = 1
+STATUS_NOT_CONVERGED = 4
+STATUS_NUMERICAL_FAILURE = 5
+
+
+@dataclass(frozen=True)
+class Result:
+    """Single-system output (reference ``_api_types.py:149-170``)."""
+
+    energy: float
+    forces: np.ndarray | None
+    converged: bool
+    iterations: int
+    energy_change: float
+    density_rms: float
+    executed_backend: str
+    basis_metadata: dict = field(default_factory=dict)
+    precision: dict | None = None
+
+
+@dataclass(frozen=True)
+class BatchItemResult:
+    index: int
+    status: int
+    status_message: str
+    energy: float
+    forces: np.ndarray | None
+    converged: bool
+    iterations: int
+    energy_change: float
+    density_rms: float
+    executed_backend: str
+    bucket_id: int
+    warm_start_used: bool = False
+    warm_start_fallback: bool = False
+    basis_metadata: dict = field(default_factory=dict)
+    precision: dict | None = None
+
+    @property
+    def succeeded(self) -> bool:
+        return self.status == STATUS_SUCCESS
+
+
+@dataclass(frozen=True)
+class BatchResult:
+    """Input-ordered results for a ragged batch; forces are never padded."""
+
+    items: tuple[BatchItemResult, ...]
+
+    @property
+    def energies(self) -> np.ndarray:
+        return np.asarray([i.energy if i.succeeded else np.nan for i in self.items], dtype=np.float64)
+
+    @property
+    def failure_indices(self) -> tuple[int, ...]:
+        return tuple(i.index for i in self.items if not i.succeeded)
+
+    @property
+    def succeeded(self) -> bool:
+        return not self.failure_indices
+
+    def raise_for_failures(self) -> None:
+        failures = [f"{i.index}: {i.status_message}" for i in self.items if not i.succeeded]
+        if failures:
+            raise RuntimeError("batched item failures: " + "; ".join(failures))
+
+
+_PRECISIONS = {"fp64": "fp64", "mixed": "mixed", "auto": "fp64"}
+
+
+class Calculator:
+    """DF-RHF energy and analytic forces on one CUDA device (coordinates in Bohr)."""
+
+    def __init__(
+        self,
+        method="rhf",
+        basis=None,
+        device: str = "cpu",
+        device_id: int = 0,
+        basis_representation: str | None = None,
+        *,
+        density_fitting="none",
+        auxiliary_basis=None,
+        density_fitting_relative_threshold: float = 1.0e-10,
+        density_fitting_memory_budget_bytes: int = 0,
+        max_iterations: int = 100,
+        energy_tolerance: float = 1.0e-10,
+        density_tolerance: float = 1.0e-8,
+        diis_history: int = 8,
+        precision: str = "fp64",
+        **unsupported,
+    ) -> None:
+        if unsupported:
+            raise NotImplementedError(f"options outside the DF-RHF CUDA path: {sorted(unsupported)}")
+        if str(method).lower() != "rhf":
+            raise NotImplementedError("only method='rhf' is served by this engine")
+        if density_fitting not in ("cuda", "auto", True):
+            raise NotImplementedError("this engine serves density_fitting='cuda' (or 'auto'/True)")
+        if device != "cuda":
+            raise NotImplementedError("this engine runs on device='cuda' only")
+        if basis is None or auxiliary_basis is None:
+            raise ValueError("basis and auxiliary_basis are required")
+        if basis_representation not in (None, "spherical", "cartesian"):
+            raise ValueError("basis_representation must be 'spherical' or 'cartesian'")
+        if precision not in _PRECISIONS:
+            raise ValueError("precision must be 'fp64', 'mixed' or 'auto'")
+        if not (0.0 <= density_fitting_relative_threshold < 1.0):
+            raise ValueError("density_fitting_relative_threshold must be in [0, 1)")
+        if max_iterations < 1 or diis_history < 1:
+            raise ValueError("max_iterations and diis_history must be positive")
+        if not torch.cuda.is_available():
+            raise RuntimeError("no CUDA device is visible")
+        _lib.lib()  # fail loudly if the native library is missing
+        self.method = "rhf"
+        self.basis = basis
+        self.auxiliary_basis = auxiliary_basis
+        self.device = torch.device("cuda", device_id)
+        self.spherical = basis_representation != "cartesian"
+        self.relative_threshold = float(density_fitting_relative_threshold)
+        self.memory_budget_bytes = int(density_fitting_memory_budget_bytes)
+        self.max_iterations = int(max_iterations)
+        self.energy_tolerance = float(energy_tolerance)
+        self.density_tolerance = float(density_tolerance)
+        self.diis_history = int(diis_history)
+        self.precision = _PRECISIONS[precision]
+        self._lock = threading.Lock()
+
+    def singlepoint(self, atoms, *, charge: int = 0, multiplicity: int = 1,
+                    properties: Iterable[str] | None = None) -> Result:
+        with self._lock:
+            batch = self.prepare_batch([list(atoms)], charges=[charge], multiplicities=[multiplicity])
+            res = batch.execute(strict=True, properties=properties)
+            batch.close()
+        item = res.items[0]
+        return Result(item.energy, item.forces, item.converged, item.iterations,
+                      item.energy_change, item.density_rms, item.executed_backend,
+                      item.basis_metadata, item.precision)
+
+    def prepare_batch(self, systems: Sequence, *, charges: Sequence[int] | None = None,
+                      multiplicities: Sequence[int] | None = None, warm_start: bool = True):
+        return PreparedBatch(self, systems, charges=charges, multiplicities=multiplicities,
+                             warm_start=warm_start)
+
+
+class PreparedBatch:
+    """Persistent plan over a ragged batch (not re-entrant; one caller at a time)."""
+
+    def __init__(self, calculator: Calculator, systems, *, charges=None, multiplicities=None,
+                 warm_start: bool = True):
+        systems = [list(s) for s in systems]
+        if not systems:
+            raise ValueError("a batch needs at least one system")
+        n = len(systems)
+        charges = [0] * n if charges is None else list(charges)
+        mults = [1] * n if multiplicities is None else list(multiplicities)
+        if len(charges) != n or len(mults) != n:
+            raise ValueError("charges and multiplicities must match the ragged batch size")
+        self._calc = calculator
+        self._closed = False
+        self._warm_start = warm_start
+        self._molecules = []
+        for atoms, q, m in zip(systems, charges, mults):
+            mol = make_molecule(atoms, calculator.basis, calculator.auxiliary_basis, q, m)
+            if m != 1 or mol.nelectron % 2:
+                raise NotImplementedError("RHF needs a closed-shell singlet (multiplicity 1, even electrons)")
+            self._molecules.append(mol)
+        # homogeneous chunks: identical (nao, naux, nocc), input order kept inside a chunk
+        groups: dict = {}
+        from . import basis as bas
+
+        for i, mol in enumerate(self._molecules):
+            key = (bas.count_functions(mol.orbital_shells, calculator.spherical),
+                   bas.count_functions(mol.aux_shells, calculator.spherical), mol.nocc)
+            groups.setdefault(key, []).append(i)
+        self._chunks = []
+        for key, idx in sorted(groups.items()):
+            self._chunks.append(Chunk([self._molecules[i] for i in idx], idx, calculator.spherical))
+        self._natoms = [len(m.atomic_numbers) for m in self._molecules]
+
+    @property
+    def size(self) -> int:
+        return len(self._molecules)
+
+    def close(self) -> None:
+        if not self._closed:
+            for c in self._chunks:
+                c.close()
+            self._closed = True
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _coords_for(self, coordinates):
+        if coordinates is None:
+            return [m.coordinates for m in self._molecules]
+        if len(coordinates) != len(self._molecules):
+            raise ValueError("coordinates must give one array per system")
+        out = []
+        for i, c in enumerate(coordinates):
+            if c is None:
+                out.append(self._molecules[i].coordinates)
+                continue
+            arr = np.asarray(c, dtype=np.float64)
+            if arr.shape != (self._natoms[i], 3):
+                raise ValueError(f"system {i}: coordinates must have shape ({self._natoms[i]}, 3)")
+            out.append(arr)
+        return out
+
+    def execute(self, coordinates=None, *, strict: bool = False,
+                properties: Iterable[str] | None = None) -> BatchResult:
+        if self._closed:
+            raise RuntimeError("prepared batch is closed")
+        props = {"energy", "forces"} if properties is None else set(properties)
+        want_forces = "forces" in props
+        coords = self._coords_for(coordinates)
+        calc = self._calc
+        items: list = [None] * len(self._molecules)
+        dev = calc.device
+        with torch.cuda.device(dev):
+            for bucket, chunk in enumerate(self._chunks):
+                xyz_h = np.concatenate([coords[i] for i in chunk.indices], axis=0)
+                finite = np.isfinite(xyz_h).all()
+                if not finite:
+                    for i in chunk.indices:
+                        items[i] = _failed(i, bucket, STATUS_INVALID_ARGUMENT, "non-finite coordinates")
+                    continue
+                xyz = torch.as_tensor(xyz_h, dtype=torch.float64).to(dev, non_blocking=True)
+                try:
+                    ints = compute_integrals(chunk.plan, xyz)
+                    out = run_scf(chunk, ints, xyz, precision=calc.precision,
+                                  max_iterations=calc.max_iterations,
+                                  energy_tolerance=calc.energy_tolerance,
+                                  density_tolerance=calc.density_tolerance,
+                                  diis_history=calc.diis_history,
+                                  relative_threshold=calc.relative_threshold)
+                    grad = df_rhf_gradient(chunk, ints, out, xyz) if want_forces else None
+                except (_lib.VqcError, FloatingPointError, torch.linalg.LinAlgError) as e:
+                    status = getattr(e, "status", STATUS_NUMERICAL_FAILURE)
+                    for i in chunk.indices:
+                        items[i] = _failed(i, bucket, status, str(e))
+                    continue
+                energy = out["energy"].cpu().numpy()
+                conv = out["converged"].cpu().numpy()
+                iters = out["iterations"].cpu().numpy()
+                de = out["energy_change"].cpu().numpy()
+                drms = out["density_rms"].cpu().numpy()
+                g = grad.cpu().numpy() if grad is not None else None
+                off = 0
+                for j, i in enumerate(chunk.indices):
+                    na = self._natoms[i]
+                    forces = None if g is None else -g[off:off + na].copy()
+                    off += na
+                    ok = bool(conv[j])
+                    items[i] = BatchItemResult(
+                        index=i,
+                        status=STATUS_SUCCESS if ok else STATUS_NOT_CONVERGED,
+                        status_message="success" if ok else "SCF did not converge",
+                        energy=float(energy[j]),
+                        forces=forces,
+                        converged=ok,
+                        iterations=int(iters[j]),
+                        energy_change=float(de[j]),
+                        density_rms=float(drms[j]),
+                        executed_backend="cuda",
+                        bucket_id=bucket,
+                        basis_metadata={"nao": chunk.nao, "naux": chunk.naux,
+                                        "metric_rank": int(out["metric"].rank[j]),
+                                        "metric_condition": float(out["metric"].condition[j])},
+                        precision={"mode": calc.precision},
+                    )
+        result = BatchResult(tuple(items))
+        if strict:
+            result.raise_for_failures()
+        return result
+
+
+def _failed(i, bucket, status, msg) -> BatchItemResult:
+    return BatchItemResult(i, status, msg, float("nan"), None, False, 0, float("nan"),
+                           float("nan"), "cuda", bucket)

@@ -1,0 +1,49 @@
+// Host-side plan object behind the opaque vqc_plan handle.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "vqc_df.h"
+#include "vqc_kernels.cuh"
+
+namespace vqc {
+
+constexpr int kMaxKernelL = 3;  // angular momentum the dispatch tables instantiate
+
+using DeviceBuffers = std::vector<void*>;
+
+struct HostShells {
+  std::vector<int> l, atom, nprim, prim_off, func_off;
+};
+
+struct Plan {
+  int nmol = 0;
+  bool sph = true;
+  int natom = 0;
+  std::vector<int> nao, naux;
+  std::vector<DevMol> mols_h;
+  HostShells orb_h, aux_h;
+  long long mat_total = 0, met_total = 0, a_total = 0;
+
+  DeviceBuffers owned;
+  int *dorb_l = nullptr, *dorb_atom = nullptr, *dorb_nprim = nullptr, *dorb_poff = nullptr,
+      *dorb_foff = nullptr;
+  double *dorb_exp = nullptr, *dorb_coef = nullptr;
+  int *daux_l = nullptr, *daux_atom = nullptr, *daux_nprim = nullptr, *daux_poff = nullptr,
+      *daux_foff = nullptr;
+  double *daux_exp = nullptr, *daux_coef = nullptr;
+  double* dcharge = nullptr;
+  DevMol* dmols = nullptr;
+  KernelArgs args{};
+
+  std::vector<ClassLaunch> cls1e, cls2c, cls3c;
+
+  int build(const vqc_batch_desc& d);
+  ~Plan();
+};
+
+int fail(int status, const std::string& msg);
+int cuda_status(cudaError_t e, const char* where);
+
+}  // namespace vqc

@@ -1,0 +1,247 @@
+"""DF-RHF driver on the GPU: integrals -> metric factor -> whitened B -> SCF.
+
+One :class:`Chunk` is a group of molecules with identical (N, X, n_occ) that
+share one native plan and run their SCF iterations as batched device work
+(the reference solves a homogeneous bucket with one batched plan,
+``src/scf/rhf.cpp:2162``; ``src/scf/fleet.cpp:27-35`` buckets the batch).
+
+SCF semantics follow ``src/scf/solver/mean_field_driver.cpp:233``: core-
+Hamiltonian guess, F = H + J - K/2, E = 1/2 tr D(H + F) + E_nn, Pulay DIIS on
+the orthogonalised commutator X^T (FDS - SDF) X with ``diis_history`` vectors,
+and convergence when |dE| < energy_tolerance, rms(dD) < density_tolerance and
+max|FDS - SDF| <= 10 * min(1e-8, density_tolerance)
+(``src/scf/cuda/scf_convergence_policy.cuh:28-37``).
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib
+from . import jk as jkmod
+from .plan import MoleculeSpec, NativePlan
+
+
+def _stream_ptr() -> int:
+    return torch.cuda.current_stream().cuda_stream
+
+
+def _dptr(t: torch.Tensor) -> int:
+    assert t.is_cuda and t.is_contiguous()
+    return t.data_ptr()
+
+
+@dataclass
+class MoleculeResult:
+    energy: float
+    forces: np.ndarray | None
+    converged: bool
+    iterations: int
+    energy_change: float
+    density_rms: float
+    status: int = 0
+    status_message: str = "success"
+    extra: dict = field(default_factory=dict)
+
+
+@dataclass
+class ChunkIntegrals:
+    s: torch.Tensor       # (nb, N, N)
+    h: torch.Tensor       # (nb, N, N)
+    metric: torch.Tensor  # (nb, X, X)
+    a_packed: torch.Tensor  # (nb, P, X)
+
+
+def compute_integrals(plan: NativePlan, xyz: torch.Tensor) -> ChunkIntegrals:
+    """Run the native integral kernels for every molecule of ``plan``."""
+    lay = plan.layout
+    nb = len(lay)
+    n, x = lay[0].nao, lay[0].naux
+    dev = xyz.device
+    s = torch.empty(plan.mat_total, dtype=torch.float64, device=dev)
+    t = torch.empty_like(s)
+    v = torch.empty_like(s)
+    m = torch.empty(plan.met_total, dtype=torch.float64, device=dev)
+    a = torch.empty(plan.a_total, dtype=torch.float64, device=dev)
+    st = _stream_ptr()
+    _lib.call("vqc_int1e", plan.handle, _dptr(xyz), _dptr(s), _dptr(t), _dptr(v), st)
+    _lib.call("vqc_int2c", plan.handle, _dptr(xyz), _dptr(m), st)
+    _lib.call("vqc_int3c", plan.handle, _dptr(xyz), _dptr(a), st)
+    p = n * (n + 1) // 2
+    return ChunkIntegrals(
+        s.view(nb, n, n), (t + v).view(nb, n, n), m.view(nb, x, x), a.view(nb, p, x)
+    )
+
+
+def nuclear_repulsion(z: torch.Tensor, xyz: torch.Tensor) -> tuple[torch.Tensor, torch.Tensor]:
+    """E_nn and its gradient for one molecule (device tensors)."""
+    d = xyz[:, None, :] - xyz[None, :, :]
+    r = torch.linalg.norm(d, dim=-1)
+    n = len(z)
+    eye = torch.eye(n, dtype=torch.bool, device=xyz.device)
+    zz = z[:, None] * z[None, :]
+    inv = torch.where(eye, torch.zeros_like(r), 1.0 / torch.where(eye, torch.ones_like(r), r))
+    e = 0.5 * (zz * inv).sum()
+    g = -((zz * inv**3)[:, :, None] * d).sum(dim=1)
+    return e, g
+
+
+@dataclass
+class MetricFactor:
+    eigenvalues: torch.Tensor   # (nb, X)
+    eigenvectors: torch.Tensor  # (nb, X, X)
+    keep: torch.Tensor          # (nb, X) bool
+    inv_sqrt: torch.Tensor      # (nb, X, X)
+    rank: list
+    condition: list
+
+
+def factor_metric(metric: torch.Tensor, relative_threshold: float = 1e-10) -> MetricFactor:
+    """FP64 eigen factor with the reference's relative cutoff.
+
+    Reference ``src/integrals/density_fitting_metric.cpp:101-154`` and its CUDA
+    counterpart ``src/scf/cuda/df_plan_setup.cpp:595-726``.
+    """
+    if not torch.isfinite(metric).all():
+        raise FloatingPointError("non-finite metric")
+    lam, vec = torch.linalg.eigh(0.5 * (metric + metric.transpose(1, 2)))
+    lmax = lam[:, -1:]
+    keep = lam > relative_threshold * lmax
+    scale = torch.where(keep, 1.0 / torch.sqrt(torch.where(keep, lam, torch.ones_like(lam))),
+                        torch.zeros_like(lam))
+    inv_sqrt = (vec * scale[:, None, :]) @ vec.transpose(1, 2)
+    rank = keep.sum(dim=1).tolist()
+    lmin = torch.where(keep, lam, torch.full_like(lam, float("inf"))).min(dim=1).values
+    cond = (lmax[:, 0] / lmin).tolist()
+    return MetricFactor(lam, vec, keep, inv_sqrt, rank, cond)
+
+
+class Chunk:
+    """A homogeneous group of molecules sharing one native plan."""
+
+    def __init__(self, molecules: list[MoleculeSpec], indices: list[int], spherical: bool = True):
+        self.molecules = molecules
+        self.indices = indices
+        self.plan = NativePlan(molecules, spherical)
+        lay = self.plan.layout
+        self.nb = len(molecules)
+        self.nao, self.naux, self.nocc = lay[0].nao, lay[0].naux, lay[0].nocc
+        for l_ in lay:
+            if (l_.nao, l_.naux, l_.nocc) != (self.nao, self.naux, self.nocc):
+                raise ValueError("a chunk must be homogeneous in (N, X, n_occ)")
+        self.natoms = [len(m.atomic_numbers) for m in molecules]
+
+    def close(self):
+        self.plan.close()
+
+
+def _orthogonalizer(s: torch.Tensor) -> torch.Tensor:
+    lam, vec = torch.linalg.eigh(s)
+    return (vec * lam.rsqrt()[:, None, :]) @ vec.transpose(1, 2)
+
+
+def _diis_extrapolate(errs: list, focks: list) -> torch.Tensor:
+    nh = len(errs)
+    e = torch.stack(errs, dim=1)  # (nb, h, N, N)
+    f = torch.stack(focks, dim=1)
+    nb = e.shape[0]
+    gram = torch.einsum("bimn,bjmn->bij", e, e)
+    bmat = -torch.ones(nb, nh + 1, nh + 1, dtype=e.dtype, device=e.device)
+    bmat[:, nh, nh] = 0.0
+    bmat[:, :nh, :nh] = gram
+    rhs = torch.zeros(nb, nh + 1, 1, dtype=e.dtype, device=e.device)
+    rhs[:, nh, 0] = -1.0
+    # scale rows for conditioning; fall back to the latest Fock on failure
+    w, info = torch.linalg.solve_ex(bmat, rhs)
+    w = w[:, :nh, 0]
+    ok = (info == 0) & torch.isfinite(w).all(dim=1)
+    ext = torch.einsum("bh,bhmn->bmn", w, f)
+    return torch.where(ok[:, None, None], ext, focks[-1])
+
+
+def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision: str = "fp64",
+            max_iterations: int = 100, energy_tolerance: float = 1e-10,
+            density_tolerance: float = 1e-8, diis_history: int = 8,
+            relative_threshold: float = 1e-10) -> dict:
+    """Batched SCF over one chunk; returns device tensors per molecule."""
+    nb, n, x, nocc = chunk.nb, chunk.nao, chunk.naux, chunk.nocc
+    dev = xyz.device
+    mf = factor_metric(ints.metric, relative_threshold)
+    b_packed = torch.bmm(ints.a_packed, mf.inv_sqrt)  # (nb, P, X) whitened, FP64
+    jk = jkmod.make_builder(precision, b_packed, n, x, nocc)
+    del b_packed
+    s, h = ints.s, ints.h
+    xo = _orthogonalizer(s)
+    enuc = []
+    off = 0
+    zs = []
+    for i, mol in enumerate(chunk.molecules):
+        na = chunk.natoms[i]
+        z = torch.as_tensor(mol.atomic_numbers, dtype=torch.float64, device=dev)
+        e, _ = nuclear_repulsion(z, xyz[off:off + na])
+        enuc.append(e)
+        zs.append(z)
+        off += na
+    enuc = torch.stack(enuc)
+
+    def diagonalize(f):
+        eps, cp = torch.linalg.eigh(xo.transpose(1, 2) @ f @ xo)
+        c = xo @ cp
+        return eps, c
+
+    eps, c = diagonalize(h)
+    d = 2.0 * c[:, :, :nocc] @ c[:, :, :nocc].transpose(1, 2)
+    active = torch.ones(nb, dtype=torch.bool, device=dev)
+    e_old = torch.full((nb,), float("nan"), dtype=torch.float64, device=dev)
+    final_e = torch.zeros(nb, dtype=torch.float64, device=dev)
+    final_de = torch.full((nb,), float("inf"), dtype=torch.float64, device=dev)
+    final_drms = torch.full((nb,), float("inf"), dtype=torch.float64, device=dev)
+    iters = torch.zeros(nb, dtype=torch.int64, device=dev)
+    converged = torch.zeros(nb, dtype=torch.bool, device=dev)
+    d_final = d.clone()
+    c_final = c.clone()
+    errs, focks = [], []
+    comm_tol = 10.0 * min(1e-8, density_tolerance)
+    for it in range(1, max_iterations + 1):
+        j, k = jk.build(d, c[:, :, :nocc])
+        f = h + j - 0.5 * k
+        energy = 0.5 * torch.einsum("bmn,bmn->b", d, h + f) + enuc
+        fds = f @ d @ s
+        comm = fds - fds.transpose(1, 2)
+        err = xo.transpose(1, 2) @ comm @ xo
+        errs.append(err)
+        focks.append(f)
+        errs, focks = errs[-diis_history:], focks[-diis_history:]
+        f_ext = _diis_extrapolate(errs, focks) if len(errs) > 1 else f
+        eps, c_new = diagonalize(f_ext)
+        d_new = 2.0 * c_new[:, :, :nocc] @ c_new[:, :, :nocc].transpose(1, 2)
+        de = (energy - e_old).abs()
+        de = torch.where(torch.isnan(de), torch.full_like(de, float("inf")), de)
+        drms = ((d_new - d) ** 2).mean(dim=(1, 2)).sqrt()
+        cmax = comm.abs().amax(dim=(1, 2))
+        done = (de < energy_tolerance) & (drms < density_tolerance) & (cmax <= comm_tol)
+        newly = done & active
+        # record the state of molecules that are still active
+        final_e = torch.where(active, energy, final_e)
+        final_de = torch.where(active, de, final_de)
+        final_drms = torch.where(active, drms, final_drms)
+        iters = torch.where(active, torch.full_like(iters, it), iters)
+        d_final = torch.where(active[:, None, None], d, d_final)
+        c_final = torch.where(active[:, None, None], c, c_final)
+        converged |= newly
+        active &= ~newly
+        e_old = energy
+        if not bool(active.any()):
+            break
+        d = torch.where(active[:, None, None], d_new, d)
+        c = torch.where(active[:, None, None], c_new, c)
+    return {
+        "energy": final_e, "converged": converged, "iterations": iters,
+        "energy_change": final_de, "density_rms": final_drms, "density": d_final,
+        "orbitals": c_final,
+        "metric": mf, "orthogonalizer": xo, "enuc": enuc, "charges": zs, "jk": jk,
+    }
