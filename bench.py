@@ -1,0 +1,321 @@
+"""DF-RHF energy + analytic forces throughput on B200 (molecules/s).
+
+Workload (synthetic, seeded): a ragged batch of 256 water clusters (H2O)_n with
+n ~ U{2..16}, each on the smallest near-cubic 3.1 A lattice holding n, random
+rigid orientations and N(0, 0.05 A) jitter; def2-SVP spherical orbitals with
+the cc-pVDZ-JKFIT auxiliary basis; energy and analytic forces for every
+molecule.  One step = one pass of the whole batch (integrals, metric, SCF,
+gradient).  The B tensor alone is tens of GB, far larger than the 126 MB L2,
+so no explicit L2 flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision mixed|fp64] [--count 256]
+
+Multi-GPU: one process per GPU (torchrun); molecules are independent, so every
+rank solves its own seeded batch with no data-path collective (weak scaling);
+the time is the max over ranks.  ``--impl reference`` times the CPU oracle port
+of the reference's DF-RHF path on this host's cores (rank 0 only).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "DF-RHF energy+force mol/s, K TFLOP/s; mixed vs FP64 GPU at |ΔE|≤1e-6 Eh"
+BASIS, AUX = "def2-svp", "cc-pvdz-jkfit"
+CPU_SAMPLE_SIZES = (2, 3, 4)
+
+
+def workload(count: int, seed: int):
+    from vibeqc_b200 import geometry
+
+    return geometry.water_cluster_batch(count, 2, 16, seed)
+
+
+def workload_sizes(count: int, seed: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    return rng.integers(2, 17, size=count)
+
+
+def cpu_reference_step(count: int, seed: int) -> dict:
+    """Oracle port on a stratified sample; power-law extrapolation to the batch."""
+    from oracle import oracle
+    from vibeqc_b200 import geometry
+
+    times = {}
+    for n in CPU_SAMPLE_SIZES:
+        atoms = geometry.water_cluster(n, np.random.default_rng([seed, 10_000 + n]))
+        t0 = time.perf_counter()
+        res = oracle.df_rhf(atoms, BASIS, AUX, forces=True)
+        times[n] = time.perf_counter() - t0
+        assert res.converged
+    ns = np.array(list(times), dtype=float)
+    ts = np.array(list(times.values()))
+    b, loga = np.polyfit(np.log(ns), np.log(ts), 1)
+    sizes = workload_sizes(count, seed)
+    total = float(np.sum(np.exp(loga) * sizes.astype(float) ** b))
+    return {"mol_per_s": count / total, "sample_seconds": float(ts.sum()), "fit_exponent": float(b),
+            "per_size_seconds": {int(k): round(v, 3) for k, v in times.items()}}
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = Path(f"/tmp/vqc_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if not self.path.exists():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        rows = [r.split(", ") for r in self.path.read_text().strip().splitlines() if r.count(",") >= 8]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for name, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(rows[0][2]),
+                "samples": len(rows), "reasons": sorted(reasons)}
+
+
+def algorithmic_model(batch) -> dict:
+    """Per-execute algorithmic work of the stages, from the batch shapes."""
+    bytes_int3c = flops_k = bytes_j = bytes_grad3c = 0.0
+    for ch in batch._chunks:
+        n, x, o, nb = ch.nao, ch.naux, ch.nocc, ch.nb
+        p = n * (n + 1) // 2
+        bytes_int3c += nb * p * x * 8.0
+        bytes_grad3c += nb * p * x * 8.0
+        flops_k += nb * (2.0 * x * n * n * o + x * o * n * (n + 1))
+        bytes_j += nb * (p * x * 4.0 + 2 * p * 8.0)
+    return {"int3c_bytes": bytes_int3c, "k_flops_per_build": flops_k, "j_bytes_per_build": bytes_j,
+            "grad3c_bytes": bytes_grad3c}
+
+
+def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
+    import torch
+
+    from vibeqc_b200 import Calculator, _lib
+    from vibeqc_b200.timing import TIMER
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    systems = workload(args.count, args.seed + rank)
+    calc = Calculator(method="rhf", basis=BASIS, auxiliary_basis=AUX, device="cuda",
+                      device_id=local_rank, density_fitting="cuda", precision=args.precision)
+    batch = calc.prepare_batch(systems)
+    xyz = batch.upload_coordinates()
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+
+    def max_over_ranks(v: float) -> float:
+        if world == 1:
+            return v
+        import torch.distributed as dist
+
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        batch.execute_device(xyz)
+    torch.cuda.synchronize()
+
+    # device-resident throughput
+    TIMER.reset()
+    TIMER.enabled = True
+    launches0 = _lib.lib().vqc_launch_count()
+    barrier()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clocks:
+        start.record()
+        for _ in range(args.steps):
+            outs = batch.execute_device(xyz)
+        end.record()
+        torch.cuda.synchronize()
+    barrier()
+    launches = (_lib.lib().vqc_launch_count() - launches0) // max(args.steps, 1)
+    TIMER.enabled = False
+    stages = TIMER.summary()
+    ms = max_over_ranks(start.elapsed_time(end))
+    value = args.count * args.steps * world / (ms / 1000.0)
+
+    # end to end through the public API with host buffers
+    coords_host = [np.asarray([p for _, p in s], dtype=np.float64) for s in systems]
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        res = batch.execute(coords_host)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1000.0)
+    e2e_value = args.count * args.steps * world / (e2e_ms / 1000.0)
+    natom = sum(len(s) for s in systems)
+    h2d = natom * 3 * 8
+    d2h = args.count * 8 * 5 + natom * 3 * 8
+    nconv = int(sum(1 for it in res.items if it.converged))
+
+    model = algorithmic_model(batch)
+    steps = args.steps
+    rl = None
+    if "int3c" in stages:
+        t_int3c = stages["int3c"]["ms"] / 1000.0 / steps
+        ach = model["int3c_bytes"] / t_int3c / 1e9
+        peaks = _peaks()
+        rl = {"kernel": "int3c (Rys 3-centre values, FP64)", "bound": "hbm", "achieved": round(ach, 1),
+              "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": round(ach / peaks["hbm_gbs"], 4),
+              "traffic": None, "peak_source": peaks["source"],
+              "note": "compute-bound FP64 Rys kernel; bytes are the FP64 tensor it writes"}
+    out = {
+        "metric": METRIC,
+        "value": round(value, 3),
+        "unit": "mol/s",
+        "n_gpus": world,
+        "steps": steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms / steps, 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "tf32x3/f32/f64",
+        "data": "synthetic",
+        "config": {"workload": f"{args.count} (H2O)n clusters, n~U{{2..16}}, def2-SVP/cc-pVDZ-JKFIT, "
+                               "energy+forces", "precision": args.precision, "molecules_per_gpu": args.count,
+                   "l2": "working set (B tensor, GBs) exceeds L2; no flush needed"},
+        "e2e": {"value": round(e2e_value, 3), "unit": "mol/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(launches),
+        "converged": nconv,
+        "clocks": clocks.summary(),
+        "roofline": rl,
+        "stages_ms_per_step": {k: round(v["ms"] / steps, 3) for k, v in stages.items()},
+    }
+    del outs
+    batch.close()
+    return out
+
+
+def _peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d["hbm_gbs"], "bf16_tflops": d["bf16_tflops"], "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="fp64")
+    ap.add_argument("--count", type=int, default=256)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        for _ in range(args.warmup):
+            pass  # the oracle has no warm state; warm-up steps are not repeated
+        vals = []
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            vals.append(cpu_reference_step(args.count, args.seed))
+        wall = time.perf_counter() - t0
+        v = float(np.median([x["mol_per_s"] for x in vals]))
+        cores = os.cpu_count()
+        line = {
+            "metric": METRIC, "value": round(v, 6), "unit": "mol/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(wall / args.steps * 1000, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"{args.count} (H2O)n clusters, n~U{{2..16}}, def2-SVP/cc-pVDZ-JKFIT, "
+                                   "energy+forces", "precision": "fp64"},
+            "cpu_baseline": {"value": round(v, 6), "unit": "mol/s", "cores": cores, "kind": "port",
+                             "sample": f"oracle DF-RHF E+F on (H2O)n n={list(CPU_SAMPLE_SIZES)}, "
+                                       f"power-law fit (exponent {vals[-1]['fit_exponent']:.2f}) "
+                                       f"extrapolated to the {args.count}-molecule size distribution"},
+            "e2e": {"value": round(v, 6), "unit": "mol/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "per_size_seconds": vals[-1]["per_size_seconds"],
+        }
+        print(json.dumps(line))
+        return 0
+
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local_rank))
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # CPU oracle before any CUDA work in this process
+        r = cpu_reference_step(args.count, args.seed)
+        cpu = {"value": round(r["mol_per_s"], 6), "unit": "mol/s", "cores": os.cpu_count(),
+               "kind": "port",
+               "sample": f"oracle DF-RHF E+F on (H2O)n n={list(CPU_SAMPLE_SIZES)} "
+                         f"({r['sample_seconds']:.1f} s), power-law fit extrapolated to the batch"}
+    out = run_ours(args, rank, world, local_rank)
+    if rank == 0:
+        out["cpu_baseline"] = cpu
+        print(json.dumps(out))
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -86,6 +86,8 @@ typedef struct {
 
 const char* vqc_last_error(void);
 uint32_t vqc_abi_version(void);
+/* Number of kernel launches this library has issued (process lifetime). */
+uint64_t vqc_launch_count(void);
 
 /* Plan over a batch topology (generativeqc_batch_prepare, generativeqc.h:1435). */
 int vqc_plan_create(const vqc_batch_desc* desc, vqc_plan** out);

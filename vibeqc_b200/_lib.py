@@ -75,6 +75,7 @@ _P = ctypes.c_void_p
 _SIGNATURES = {
     "vqc_last_error": ([], ctypes.c_char_p),
     "vqc_abi_version": ([], ctypes.c_uint32),
+    "vqc_launch_count": ([], ctypes.c_uint64),
     "vqc_plan_create": ([ctypes.POINTER(BatchDesc), ctypes.POINTER(_P)], ctypes.c_int),
     "vqc_plan_destroy": ([_P], ctypes.c_int),
     "vqc_plan_totals": ([_P, _P, _P, _P, _P], ctypes.c_int),

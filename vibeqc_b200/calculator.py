@@ -199,9 +199,17 @@ class PreparedBatch:
             key = (bas.count_functions(mol.orbital_shells, calculator.spherical),
                    bas.count_functions(mol.aux_shells, calculator.spherical), mol.nocc)
             groups.setdefault(key, []).append(i)
+        budget = calculator.memory_budget_bytes
+        if budget <= 0:
+            budget = int(0.55 * torch.cuda.get_device_properties(calculator.device).total_memory)
         self._chunks = []
-        for key, idx in sorted(groups.items()):
-            self._chunks.append(Chunk([self._molecules[i] for i in idx], idx, calculator.spherical))
+        for (nao, naux, _), idx in sorted(groups.items()):
+            per_mol = _device_bytes_per_molecule(nao, naux, calculator.precision)
+            limit = max(1, budget // per_mol)
+            for s in range(0, len(idx), limit):
+                part = idx[s:s + limit]
+                self._chunks.append(Chunk([self._molecules[i] for i in part], part,
+                                          calculator.spherical))
         self._natoms = [len(m.atomic_numbers) for m in self._molecules]
 
     @property
@@ -236,6 +244,37 @@ class PreparedBatch:
             out.append(arr)
         return out
 
+    def _run_chunk(self, chunk, xyz: torch.Tensor, want_forces: bool):
+        """Integrals, SCF and (optionally) the gradient of one chunk, all on device."""
+        calc = self._calc
+        ints = compute_integrals(chunk.plan, xyz)
+        out = run_scf(chunk, ints, xyz, precision=calc.precision,
+                      max_iterations=calc.max_iterations,
+                      energy_tolerance=calc.energy_tolerance,
+                      density_tolerance=calc.density_tolerance,
+                      diis_history=calc.diis_history,
+                      relative_threshold=calc.relative_threshold)
+        grad = df_rhf_gradient(chunk, ints, out, xyz) if want_forces else None
+        return out, grad
+
+    def upload_coordinates(self, coordinates=None) -> list:
+        """Per-chunk device coordinate tensors (Bohr) for :meth:`execute_device`."""
+        coords = self._coords_for(coordinates)
+        return [
+            torch.as_tensor(np.concatenate([coords[i] for i in c.indices], axis=0),
+                            dtype=torch.float64).to(self._calc.device, non_blocking=True)
+            for c in self._chunks
+        ]
+
+    def execute_device(self, xyz_chunks: list, *, want_forces: bool = True) -> list:
+        """Device-resident execution: inputs and outputs stay in HBM.
+
+        Returns, per chunk, ``(scf_output_dict, gradient_or_None)`` with device
+        tensors; no host copies are made.
+        """
+        with torch.cuda.device(self._calc.device):
+            return [self._run_chunk(c, x, want_forces) for c, x in zip(self._chunks, xyz_chunks)]
+
     def execute(self, coordinates=None, *, strict: bool = False,
                 properties: Iterable[str] | None = None) -> BatchResult:
         if self._closed:
@@ -249,21 +288,13 @@ class PreparedBatch:
         with torch.cuda.device(dev):
             for bucket, chunk in enumerate(self._chunks):
                 xyz_h = np.concatenate([coords[i] for i in chunk.indices], axis=0)
-                finite = np.isfinite(xyz_h).all()
-                if not finite:
+                if not np.isfinite(xyz_h).all():
                     for i in chunk.indices:
                         items[i] = _failed(i, bucket, STATUS_INVALID_ARGUMENT, "non-finite coordinates")
                     continue
                 xyz = torch.as_tensor(xyz_h, dtype=torch.float64).to(dev, non_blocking=True)
                 try:
-                    ints = compute_integrals(chunk.plan, xyz)
-                    out = run_scf(chunk, ints, xyz, precision=calc.precision,
-                                  max_iterations=calc.max_iterations,
-                                  energy_tolerance=calc.energy_tolerance,
-                                  density_tolerance=calc.density_tolerance,
-                                  diis_history=calc.diis_history,
-                                  relative_threshold=calc.relative_threshold)
-                    grad = df_rhf_gradient(chunk, ints, out, xyz) if want_forces else None
+                    out, grad = self._run_chunk(chunk, xyz, want_forces)
                 except (_lib.VqcError, FloatingPointError, torch.linalg.LinAlgError) as e:
                     status = getattr(e, "status", STATUS_NUMERICAL_FAILURE)
                     for i in chunk.indices:
@@ -302,6 +333,13 @@ class PreparedBatch:
         if strict:
             result.raise_for_failures()
         return result
+
+
+def _device_bytes_per_molecule(nao: int, naux: int, precision: str) -> int:
+    """Peak device bytes one molecule holds during a chunk (integrals to gradient)."""
+    p = nao * (nao + 1) // 2
+    b_bytes = 8 if precision == "fp64" else 4
+    return int(8 * p * naux * 2 + b_bytes * nao * nao * naux + 8 * nao * nao * naux + 64 * nao * nao)
 
 
 def _failed(i, bucket, status, msg) -> BatchItemResult:

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -19,11 +20,14 @@
 namespace vqc {
 
 thread_local std::string g_last_error;
+std::atomic<unsigned long long> g_launches{0};
 
 int fail(int status, const std::string& msg) {
   g_last_error = msg;
   return status;
 }
+
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 int cuda_status(cudaError_t e, const char* where) {
   if (e == cudaSuccess) return VQC_STATUS_SUCCESS;
@@ -237,6 +241,7 @@ extern "C" {
 
 const char* vqc_last_error(void) { return g_last_error.c_str(); }
 uint32_t vqc_abi_version(void) { return VQC_ABI_VERSION; }
+uint64_t vqc_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
 int vqc_plan_create(const vqc_batch_desc* desc, vqc_plan** out) {
   VQC_GUARD_BEGIN
@@ -294,6 +299,7 @@ static int run_classes(Plan* p, const std::vector<ClassLaunch>& list,
   for (const ClassLaunch& cl : list) {
     if (!dispatch(cl, k, p->sph, st))
       return fail(VQC_STATUS_INVALID_ARGUMENT, std::string(what) + ": unsupported class");
+    g_launches.fetch_add(1, std::memory_order_relaxed);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_status(e, what);
   }

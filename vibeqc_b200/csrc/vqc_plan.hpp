@@ -44,6 +44,7 @@ struct Plan {
 };
 
 int fail(int status, const std::string& msg);
+void count_launch();
 int cuda_status(cudaError_t e, const char* where);
 
 }  // namespace vqc

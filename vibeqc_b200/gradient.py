@@ -24,6 +24,7 @@ import torch
 
 from . import _lib
 from .jk import unpack_index
+from .timing import TIMER
 
 
 def _packed_rows(n: int, device) -> torch.Tensor:
@@ -52,6 +53,8 @@ def df_rhf_gradient(chunk, ints, scf_out: dict, xyz: torch.Tensor) -> torch.Tens
     dens = 2.0 * c @ c.transpose(1, 2)
     wdens = 2.0 * (c * eps[:, None, :o]) @ c.transpose(1, 2)
 
+    wctx = TIMER.stage("grad_weights")
+    wctx.__enter__()
     b = jk.whitened_fp64()  # (nb, N*N, X) whitened, FP64
     rho_w = torch.bmm(dens.reshape(nb, 1, n * n), b)[:, 0, :]  # (nb, X)
     cvec = torch.bmm(mf.inv_sqrt, rho_w[:, :, None])[:, :, 0]  # raw-basis c = Minv rho
@@ -72,13 +75,17 @@ def df_rhf_gradient(chunk, ints, scf_out: dict, xyz: torch.Tensor) -> torch.Tens
     gflat = gam.reshape(nb, x, o * o)
     mbar = -0.5 * cvec[:, :, None] * cvec[:, None, :] + torch.bmm(gflat, gflat.transpose(1, 2))
 
+    wctx.__exit__(None, None, None)
     grad = torch.zeros(plan.natom * 3, dtype=torch.float64, device=dev)
     st = torch.cuda.current_stream().cuda_stream
-    _lib.call("vqc_grad1e", plan.handle, xyz.data_ptr(), dens.contiguous().data_ptr(),
-              wdens.contiguous().data_ptr(), grad.data_ptr(), st)
-    _lib.call("vqc_grad3c", plan.handle, xyz.data_ptr(), abar.data_ptr(), grad.data_ptr(), st)
-    _lib.call("vqc_grad2c", plan.handle, xyz.data_ptr(), mbar.contiguous().data_ptr(),
-              grad.data_ptr(), st)
+    with TIMER.stage("grad1e"):
+        _lib.call("vqc_grad1e", plan.handle, xyz.data_ptr(), dens.contiguous().data_ptr(),
+                  wdens.contiguous().data_ptr(), grad.data_ptr(), st)
+    with TIMER.stage("grad3c"):
+        _lib.call("vqc_grad3c", plan.handle, xyz.data_ptr(), abar.data_ptr(), grad.data_ptr(), st)
+    with TIMER.stage("grad2c"):
+        _lib.call("vqc_grad2c", plan.handle, xyz.data_ptr(), mbar.contiguous().data_ptr(),
+                  grad.data_ptr(), st)
     grad = grad.view(-1, 3)
     from .scf import nuclear_repulsion
 

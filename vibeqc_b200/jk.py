@@ -10,6 +10,8 @@ from __future__ import annotations
 
 import torch
 
+from .timing import TIMER
+
 
 def unpack_index(n: int, device) -> torch.Tensor:
     mu = torch.arange(n, device=device)
@@ -32,13 +34,15 @@ class FP64Builder:
     def build(self, d: torch.Tensor, c_occ: torch.Tensor):
         nb, n, x, o = d.shape[0], self.n, self.x, self.nocc
         b = self.b
-        rho = torch.bmm(d.reshape(nb, 1, n * n), b)  # (nb, 1, X)
-        j = torch.bmm(b, rho.transpose(1, 2)).reshape(nb, n, n)
-        # U[b, mu, Q, i] = sum_nu B[mu, nu, Q] C[nu, i]
-        b4 = b.view(nb, n, n, x)
-        u = torch.matmul(b4.transpose(2, 3), c_occ[:, None, :, :])  # (nb, N, X, o)
-        u = u.reshape(nb, n, x * o)
-        k = 2.0 * torch.bmm(u, u.transpose(1, 2))
+        with TIMER.stage("J_fp64"):
+            rho = torch.bmm(d.reshape(nb, 1, n * n), b)  # (nb, 1, X)
+            j = torch.bmm(b, rho.transpose(1, 2)).reshape(nb, n, n)
+        with TIMER.stage("K_fp64"):
+            # U[b, mu, Q, i] = sum_nu B[mu, nu, Q] C[nu, i]
+            b4 = b.view(nb, n, n, x)
+            u = torch.matmul(b4.transpose(2, 3), c_occ[:, None, :, :])  # (nb, N, X, o)
+            u = u.reshape(nb, n, x * o)
+            k = 2.0 * torch.bmm(u, u.transpose(1, 2))
         self.nbuild += 1
         return j, k
 

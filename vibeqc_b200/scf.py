@@ -24,6 +24,7 @@ import torch
 from . import _lib
 from . import jk as jkmod
 from .plan import MoleculeSpec, NativePlan
+from .timing import TIMER
 
 
 def _stream_ptr() -> int:
@@ -68,9 +69,12 @@ def compute_integrals(plan: NativePlan, xyz: torch.Tensor) -> ChunkIntegrals:
     m = torch.empty(plan.met_total, dtype=torch.float64, device=dev)
     a = torch.empty(plan.a_total, dtype=torch.float64, device=dev)
     st = _stream_ptr()
-    _lib.call("vqc_int1e", plan.handle, _dptr(xyz), _dptr(s), _dptr(t), _dptr(v), st)
-    _lib.call("vqc_int2c", plan.handle, _dptr(xyz), _dptr(m), st)
-    _lib.call("vqc_int3c", plan.handle, _dptr(xyz), _dptr(a), st)
+    with TIMER.stage("int1e"):
+        _lib.call("vqc_int1e", plan.handle, _dptr(xyz), _dptr(s), _dptr(t), _dptr(v), st)
+    with TIMER.stage("int2c"):
+        _lib.call("vqc_int2c", plan.handle, _dptr(xyz), _dptr(m), st)
+    with TIMER.stage("int3c"):
+        _lib.call("vqc_int3c", plan.handle, _dptr(xyz), _dptr(a), st)
     p = n * (n + 1) // 2
     return ChunkIntegrals(
         s.view(nb, n, n), (t + v).view(nb, n, n), m.view(nb, x, x), a.view(nb, p, x)
@@ -170,10 +174,12 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
     """Batched SCF over one chunk; returns device tensors per molecule."""
     nb, n, x, nocc = chunk.nb, chunk.nao, chunk.naux, chunk.nocc
     dev = xyz.device
-    mf = factor_metric(ints.metric, relative_threshold)
-    b_packed = torch.bmm(ints.a_packed, mf.inv_sqrt)  # (nb, P, X) whitened, FP64
-    jk = jkmod.make_builder(precision, b_packed, n, x, nocc)
-    del b_packed
+    with TIMER.stage("metric_factor"):
+        mf = factor_metric(ints.metric, relative_threshold)
+    with TIMER.stage("whiten"):
+        b_packed = torch.bmm(ints.a_packed, mf.inv_sqrt)  # (nb, P, X) whitened, FP64
+        jk = jkmod.make_builder(precision, b_packed, n, x, nocc)
+        del b_packed
     s, h = ints.s, ints.h
     xo = _orthogonalizer(s)
     enuc = []
@@ -208,6 +214,8 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
     comm_tol = 10.0 * min(1e-8, density_tolerance)
     for it in range(1, max_iterations + 1):
         j, k = jk.build(d, c[:, :, :nocc])
+        TIMER_ctx = TIMER.stage("scf_other")
+        TIMER_ctx.__enter__()
         f = h + j - 0.5 * k
         energy = 0.5 * torch.einsum("bmn,bmn->b", d, h + f) + enuc
         fds = f @ d @ s
@@ -236,9 +244,11 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
         active &= ~newly
         e_old = energy
         if not bool(active.any()):
+            TIMER_ctx.__exit__(None, None, None)
             break
         d = torch.where(active[:, None, None], d_new, d)
         c = torch.where(active[:, None, None], c_new, c)
+        TIMER_ctx.__exit__(None, None, None)
     return {
         "energy": final_e, "converged": converged, "iterations": iters,
         "energy_change": final_de, "density_rms": final_drms, "density": d_final,
