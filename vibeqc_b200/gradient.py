@@ -41,40 +41,35 @@ def df_rhf_gradient(chunk, ints, scf_out: dict, xyz: torch.Tensor) -> torch.Tens
     mf = scf_out["metric"]
     if any(r < x for r in mf.rank):
         raise _lib.VqcError(5, "analytic forces need a full-rank auxiliary metric")
-    d0 = scf_out["density"]
+    dens = scf_out["density"]
+    c = scf_out["orbitals"]  # AO occupied factor, dens = 2 c c^T
+    f = scf_out["fock"]
     jk = scf_out["jk"]
-    # final Fock at the returned density -> orbitals, energy-weighted density
-    c_prev = scf_out.get("orbitals")
-    j, k = jk.build(d0, c_prev[:, :, :o]) if c_prev is not None else jk.build(d0, None)
-    f = ints.h + j - 0.5 * k
-    xo = scf_out["orthogonalizer"]
-    eps, cp = torch.linalg.eigh(xo.transpose(1, 2) @ f @ xo)
-    c = (xo @ cp)[:, :, :o]
-    dens = 2.0 * c @ c.transpose(1, 2)
-    wdens = 2.0 * (c * eps[:, None, :o]) @ c.transpose(1, 2)
+    # energy-weighted density of the converged closed shell: W = D F D / 2
+    wdens = 0.5 * dens @ f @ dens
 
     wctx = TIMER.stage("grad_weights")
     wctx.__enter__()
     b = jk.whitened_fp64()  # (nb, N*N, X) whitened, FP64
-    rho_w = torch.bmm(dens.reshape(nb, 1, n * n), b)[:, 0, :]  # (nb, X)
-    cvec = torch.bmm(mf.inv_sqrt, rho_w[:, :, None])[:, :, 0]  # raw-basis c = Minv rho
-    # B[ij, Q]: half transform then quarter transform
-    b4 = b.view(nb, n, n, x)
-    u = torch.matmul(b4.transpose(2, 3), c[:, None, :, :])  # (nb, N(mu), X, o(j))
-    bij = torch.einsum("bmi,bmqj->bqij", c, u)  # (nb, X, o, o)
-    del u
-    gam = torch.bmm(mf.inv_sqrt, bij.reshape(nb, x, o * o)).view(nb, x, o, o)
-    # Abar (full square), then packed rows
-    t1 = torch.einsum("bnj,bpij->bpin", c, gam)  # (nb, X, o, N)
-    abar_sq = torch.einsum("bmi,bpin->bmnp", c, t1)  # (nb, N, N, X)
-    del t1
-    abar_sq = dens[:, :, :, None] * cvec[:, None, None, :] - 2.0 * abar_sq
     rows = _packed_rows(n, dev)
-    abar = abar_sq.reshape(nb, n * n, x)[:, rows, :].contiguous()
-    del abar_sq
-    gflat = gam.reshape(nb, x, o * o)
-    mbar = -0.5 * cvec[:, :, None] * cvec[:, None, :] + torch.bmm(gflat, gflat.transpose(1, 2))
-
+    abar = torch.empty(nb, rows.numel(), x, dtype=torch.float64, device=dev)
+    mbar = torch.empty(nb, x, x, dtype=torch.float64, device=dev)
+    for m in range(nb):  # per molecule: bounded temporaries
+        bm = b[m]
+        rho_w = dens[m].reshape(1, n * n) @ bm  # (1, X)
+        cvec = (mf.inv_sqrt[m] @ rho_w[0])  # raw-basis c = Minv rho
+        u = torch.matmul(bm.view(n, n, x).transpose(1, 2), c[m])  # (N(mu), X, o(j))
+        bij = torch.einsum("mi,mqj->qij", c[m], u)  # (X, o, o)
+        del u
+        gam = (mf.inv_sqrt[m] @ bij.reshape(x, o * o)).view(x, o, o)
+        t1 = torch.einsum("nj,pij->inp", c[m], gam).reshape(o, n * x)  # (o, N*X)
+        sq = (c[m] @ t1).view(n * n, x)  # (N*N, X) = sum_i C[mu i] T[i, nu, P]
+        del t1
+        sq = dens[m].reshape(n * n, 1) * cvec[None, :] - 2.0 * sq
+        abar[m] = sq[rows]
+        del sq
+        gflat = gam.reshape(x, o * o)
+        mbar[m] = -0.5 * torch.outer(cvec, cvec) + gflat @ gflat.T
     wctx.__exit__(None, None, None)
     grad = torch.zeros(plan.natom * 3, dtype=torch.float64, device=dev)
     st = torch.cuda.current_stream().cuda_stream

@@ -96,23 +96,43 @@ def nuclear_repulsion(z: torch.Tensor, xyz: torch.Tensor) -> tuple[torch.Tensor,
 
 @dataclass
 class MetricFactor:
-    eigenvalues: torch.Tensor   # (nb, X)
-    eigenvectors: torch.Tensor  # (nb, X, X)
-    keep: torch.Tensor          # (nb, X) bool
-    inv_sqrt: torch.Tensor      # (nb, X, X)
+    eigenvalues: torch.Tensor | None   # (nb, X); None for the Cholesky factor
+    eigenvectors: torch.Tensor | None  # (nb, X, X)
+    keep: torch.Tensor                 # (nb, X) bool
+    inv_sqrt: torch.Tensor             # (nb, X, X) whitening W with W W^T = M^+
     rank: list
-    condition: list
+    condition: list                    # exact (eigen) or certified upper bound (Cholesky)
+    kind: str = "eigen"
 
 
 def factor_metric(metric: torch.Tensor, relative_threshold: float = 1e-10) -> MetricFactor:
-    """FP64 eigen factor with the reference's relative cutoff.
+    """FP64 whitening factor W (W W^T = M^+) with the reference's relative cutoff.
 
-    Reference ``src/integrals/density_fitting_metric.cpp:101-154`` and its CUDA
-    counterpart ``src/scf/cuda/df_plan_setup.cpp:595-726``.
+    The reference keeps eigenvectors with lambda > rel * lambda_max
+    (``src/integrals/density_fitting_metric.cpp:101-154``; CUDA
+    ``src/scf/cuda/df_plan_setup.cpp:595-726``).  When a rigorous certificate
+    shows that no eigenvalue is cut -- lambda_min >= 1/tr(M^-1) exceeds
+    rel * max_i sum_j |M_ij| >= rel * lambda_max -- the eigen factor and the
+    Cholesky factor W = L^-T span the same fitting space and give identical
+    J, K, energies and forces, so the cheaper Cholesky factor is used.
+    Otherwise the eigen factor with the cutoff is formed.
     """
     if not torch.isfinite(metric).all():
         raise FloatingPointError("non-finite metric")
-    lam, vec = torch.linalg.eigh(0.5 * (metric + metric.transpose(1, 2)))
+    m = 0.5 * (metric + metric.transpose(1, 2))
+    nb, x, _ = m.shape
+    l, info = torch.linalg.cholesky_ex(m)
+    if bool((info == 0).all()):
+        eye = torch.eye(x, dtype=m.dtype, device=m.device).expand(nb, x, x)
+        linv = torch.linalg.solve_triangular(l, eye, upper=False)
+        lam_min_lower = 1.0 / (linv * linv).sum(dim=(1, 2))
+        lam_max_upper = m.abs().sum(dim=2).max(dim=1).values
+        if bool((lam_min_lower > relative_threshold * lam_max_upper).all()):
+            w = linv.transpose(1, 2).contiguous()
+            keep = torch.ones(nb, x, dtype=torch.bool, device=m.device)
+            cond = (lam_max_upper / lam_min_lower).tolist()
+            return MetricFactor(None, None, keep, w, [x] * nb, cond, "cholesky")
+    lam, vec = torch.linalg.eigh(m)
     lmax = lam[:, -1:]
     keep = lam > relative_threshold * lmax
     scale = torch.where(keep, 1.0 / torch.sqrt(torch.where(keep, lam, torch.ones_like(lam))),
@@ -121,7 +141,7 @@ def factor_metric(metric: torch.Tensor, relative_threshold: float = 1e-10) -> Me
     rank = keep.sum(dim=1).tolist()
     lmin = torch.where(keep, lam, torch.full_like(lam, float("inf"))).min(dim=1).values
     cond = (lmax[:, 0] / lmin).tolist()
-    return MetricFactor(lam, vec, keep, inv_sqrt, rank, cond)
+    return MetricFactor(lam, vec, keep, inv_sqrt, rank, cond, "eigen")
 
 
 class Chunk:
@@ -144,8 +164,53 @@ class Chunk:
 
 
 def _orthogonalizer(s: torch.Tensor) -> torch.Tensor:
+    """X with X^T S X = I: inverse transposed Cholesky factor (eigen fallback)."""
+    l, info = torch.linalg.cholesky_ex(s)
+    if bool((info == 0).all()):
+        eye = torch.eye(s.shape[-1], dtype=s.dtype, device=s.device).expand_as(s)
+        return torch.linalg.solve_triangular(l, eye, upper=False).transpose(1, 2)
     lam, vec = torch.linalg.eigh(s)
     return (vec * lam.rsqrt()[:, None, :]) @ vec.transpose(1, 2)
+
+
+def purify_sp2(fo: torch.Tensor, nocc: int, max_steps: int = 100, tol: float = 1e-11) -> torch.Tensor:
+    """Projector onto the lowest ``nocc`` eigenvectors of symmetric ``fo``.
+
+    Second-order spectral projection (Niklasson, Phys. Rev. B 66, 155115
+    (2002)): map the spectrum into [0, 1] with Gershgorin bounds, then apply
+    X <- X^2 or X <- 2X - X^2, whichever moves tr X toward ``nocc``, until
+    tr(X) - tr(X^2) < tol.  Only batched GEMMs; no eigensolver.
+    """
+    nb, n, _ = fo.shape
+    diag = torch.diagonal(fo, dim1=1, dim2=2)
+    radius = fo.abs().sum(dim=2) - diag.abs()
+    emin = (diag - radius).min(dim=1).values
+    emax = (diag + radius).max(dim=1).values
+    eye = torch.eye(n, dtype=fo.dtype, device=fo.device)
+    x = (emax[:, None, None] * eye - fo) / (emax - emin)[:, None, None]
+    target = float(nocc)
+    for step in range(max_steps):
+        x2 = torch.bmm(x, x)
+        tr = torch.diagonal(x, dim1=1, dim2=2).sum(dim=1)
+        tr2 = torch.diagonal(x2, dim1=1, dim2=2).sum(dim=1)
+        err = (tr - tr2).abs()
+        if step % 4 == 3 and bool((err < tol).all()):
+            break
+        square = (tr2 - target).abs() < (2.0 * tr - tr2 - target).abs()
+        x = torch.where(square[:, None, None], x2, 2.0 * x - x2)
+    return 0.5 * (x + x.transpose(1, 2))
+
+
+def occupied_factor(proj: torch.Tensor, guess: torch.Tensor) -> torch.Tensor:
+    """Orthonormal basis of range(proj) (rank = guess columns) by Cholesky-QR2 of proj @ guess."""
+    y = torch.bmm(proj, guess)
+    for _ in range(2):
+        g = torch.bmm(y.transpose(1, 2), y)
+        u, info = torch.linalg.cholesky_ex(g, upper=True)
+        if not bool((info == 0).all()):
+            raise FloatingPointError("occupied-space factorisation failed")
+        y = torch.linalg.solve_triangular(u, y, upper=True, left=False)
+    return y
 
 
 def _diis_extrapolate(errs: list, focks: list) -> torch.Tensor:
@@ -178,6 +243,7 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
         mf = factor_metric(ints.metric, relative_threshold)
     with TIMER.stage("whiten"):
         b_packed = torch.bmm(ints.a_packed, mf.inv_sqrt)  # (nb, P, X) whitened, FP64
+        ints.a_packed = None  # the raw tensor is not needed after whitening
         jk = jkmod.make_builder(precision, b_packed, n, x, nocc)
         del b_packed
     s, h = ints.s, ints.h
@@ -194,13 +260,18 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
         off += na
     enuc = torch.stack(enuc)
 
-    def diagonalize(f):
-        eps, cp = torch.linalg.eigh(xo.transpose(1, 2) @ f @ xo)
-        c = xo @ cp
-        return eps, c
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(1234)
+    guess = torch.randn(nb, n, nocc, dtype=torch.float64, device=dev, generator=gen)
 
-    eps, c = diagonalize(h)
-    d = 2.0 * c[:, :, :nocc] @ c[:, :, :nocc].transpose(1, 2)
+    def density_from(f, guess):
+        with TIMER.stage("purify"):
+            proj = purify_sp2(xo.transpose(1, 2) @ f @ xo, nocc)
+            co = occupied_factor(proj, guess)  # orthonormal, orthogonal basis
+        return 2.0 * (xo @ proj @ xo.transpose(1, 2)), co
+
+    d, co = density_from(h, guess)
+    c = xo @ co  # AO occupied factor, D = 2 C C^T
     active = torch.ones(nb, dtype=torch.bool, device=dev)
     e_old = torch.full((nb,), float("nan"), dtype=torch.float64, device=dev)
     final_e = torch.zeros(nb, dtype=torch.float64, device=dev)
@@ -210,10 +281,11 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
     converged = torch.zeros(nb, dtype=torch.bool, device=dev)
     d_final = d.clone()
     c_final = c.clone()
+    f_final = torch.zeros_like(d)
     errs, focks = [], []
     comm_tol = 10.0 * min(1e-8, density_tolerance)
     for it in range(1, max_iterations + 1):
-        j, k = jk.build(d, c[:, :, :nocc])
+        j, k = jk.build(d, c)
         TIMER_ctx = TIMER.stage("scf_other")
         TIMER_ctx.__enter__()
         f = h + j - 0.5 * k
@@ -225,8 +297,11 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
         focks.append(f)
         errs, focks = errs[-diis_history:], focks[-diis_history:]
         f_ext = _diis_extrapolate(errs, focks) if len(errs) > 1 else f
-        eps, c_new = diagonalize(f_ext)
-        d_new = 2.0 * c_new[:, :, :nocc] @ c_new[:, :, :nocc].transpose(1, 2)
+        TIMER_ctx.__exit__(None, None, None)
+        d_new, co = density_from(f_ext, co)
+        TIMER_ctx = TIMER.stage("scf_other")
+        TIMER_ctx.__enter__()
+        c_new = xo @ co
         de = (energy - e_old).abs()
         de = torch.where(torch.isnan(de), torch.full_like(de, float("inf")), de)
         drms = ((d_new - d) ** 2).mean(dim=(1, 2)).sqrt()
@@ -240,6 +315,7 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
         iters = torch.where(active, torch.full_like(iters, it), iters)
         d_final = torch.where(active[:, None, None], d, d_final)
         c_final = torch.where(active[:, None, None], c, c_final)
+        f_final = torch.where(active[:, None, None], f, f_final)
         converged |= newly
         active &= ~newly
         e_old = energy
@@ -252,6 +328,6 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
     return {
         "energy": final_e, "converged": converged, "iterations": iters,
         "energy_change": final_de, "density_rms": final_drms, "density": d_final,
-        "orbitals": c_final,
+        "orbitals": c_final, "fock": f_final,
         "metric": mf, "orthogonalizer": xo, "enuc": enuc, "charges": zs, "jk": jk,
     }
