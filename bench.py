@@ -29,6 +29,7 @@ from pathlib import Path
 
 import numpy as np
 
+os.environ.setdefault("PYTORCH_CUDA_ALLOC_CONF", "expandable_segments:True")
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 

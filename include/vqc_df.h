@@ -124,6 +124,17 @@ int vqc_grad2c(vqc_plan* plan, const double* xyz, const double* mbar, double* gr
 int vqc_grad1e(vqc_plan* plan, const double* xyz, const double* dens, const double* wdens,
                double* grad, void* stream);
 
+/*
+ * One SP2 purification step for nmol molecules of one size n (row-major n*n
+ * blocks, contiguous): xout = x2 or 2x - x2 per molecule (x2 = x x), chosen to
+ * move tr x toward nocc; molecules with |tr x - tr x2| < tol are copied and
+ * flagged in done[nmol].  Replaces the batched Fock eigensolve of the
+ * reference's device SCF loop (src/scf/cuda/df_scf_library.cpp) for the
+ * density update.
+ */
+int vqc_sp2_update(const double* x, const double* x2, double* xout, int32_t nmol, int32_t n,
+                   double nocc, double tol, int32_t* done, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

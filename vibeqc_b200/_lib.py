@@ -86,6 +86,8 @@ _SIGNATURES = {
     "vqc_grad3c": ([_P, _P, _P, _P, _P], ctypes.c_int),
     "vqc_grad2c": ([_P, _P, _P, _P, _P], ctypes.c_int),
     "vqc_grad1e": ([_P, _P, _P, _P, _P, _P], ctypes.c_int),
+    "vqc_sp2_update": ([_P, _P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+                        ctypes.c_double, _P, _P], ctypes.c_int),
 }
 
 _lib = None

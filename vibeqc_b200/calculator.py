@@ -201,7 +201,7 @@ class PreparedBatch:
             groups.setdefault(key, []).append(i)
         budget = calculator.memory_budget_bytes
         if budget <= 0:
-            budget = int(0.55 * torch.cuda.get_device_properties(calculator.device).total_memory)
+            budget = int(0.6 * torch.cuda.get_device_properties(calculator.device).total_memory)
         self._chunks = []
         for (nao, naux, _), idx in sorted(groups.items()):
             per_mol = _device_bytes_per_molecule(nao, naux, calculator.precision)
@@ -338,8 +338,8 @@ class PreparedBatch:
 def _device_bytes_per_molecule(nao: int, naux: int, precision: str) -> int:
     """Peak device bytes one molecule holds during a chunk (integrals to gradient)."""
     p = nao * (nao + 1) // 2
-    b_bytes = 8 if precision == "fp64" else 4
-    return int(8 * p * naux * 2 + b_bytes * nao * nao * naux + 8 * nao * nao * naux + 64 * nao * nao)
+    per_px = 26 if precision == "fp64" else 20  # packed A/B + full B + packed Abar
+    return int(per_px * p * naux + 64 * nao * nao)
 
 
 def _failed(i, bucket, status, msg) -> BatchItemResult:

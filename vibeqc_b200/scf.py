@@ -173,13 +173,16 @@ def _orthogonalizer(s: torch.Tensor) -> torch.Tensor:
     return (vec * lam.rsqrt()[:, None, :]) @ vec.transpose(1, 2)
 
 
-def purify_sp2(fo: torch.Tensor, nocc: int, max_steps: int = 100, tol: float = 1e-11) -> torch.Tensor:
+def purify_sp2(fo: torch.Tensor, nocc: int, max_steps: int = 96, tol: float = 1e-11,
+               check_every: int = 8) -> torch.Tensor:
     """Projector onto the lowest ``nocc`` eigenvectors of symmetric ``fo``.
 
     Second-order spectral projection (Niklasson, Phys. Rev. B 66, 155115
     (2002)): map the spectrum into [0, 1] with Gershgorin bounds, then apply
     X <- X^2 or X <- 2X - X^2, whichever moves tr X toward ``nocc``, until
-    tr(X) - tr(X^2) < tol.  Only batched GEMMs; no eigensolver.
+    tr(X) - tr(X^2) < tol.  Per step: one batched GEMM and one native update
+    kernel (vqc_sp2_update); convergence flags stay on the device and are read
+    every ``check_every`` steps.
     """
     nb, n, _ = fo.shape
     diag = torch.diagonal(fo, dim1=1, dim2=2)
@@ -187,30 +190,45 @@ def purify_sp2(fo: torch.Tensor, nocc: int, max_steps: int = 100, tol: float = 1
     emin = (diag - radius).min(dim=1).values
     emax = (diag + radius).max(dim=1).values
     eye = torch.eye(n, dtype=fo.dtype, device=fo.device)
-    x = (emax[:, None, None] * eye - fo) / (emax - emin)[:, None, None]
-    target = float(nocc)
+    x = ((emax[:, None, None] * eye - fo) / (emax - emin)[:, None, None]).contiguous()
+    x2 = torch.empty_like(x)
+    xn = torch.empty_like(x)
+    done = torch.zeros(nb, dtype=torch.int32, device=fo.device)
+    st = torch.cuda.current_stream().cuda_stream
     for step in range(max_steps):
-        x2 = torch.bmm(x, x)
-        tr = torch.diagonal(x, dim1=1, dim2=2).sum(dim=1)
-        tr2 = torch.diagonal(x2, dim1=1, dim2=2).sum(dim=1)
-        err = (tr - tr2).abs()
-        if step % 4 == 3 and bool((err < tol).all()):
+        torch.bmm(x, x, out=x2)
+        _lib.call("vqc_sp2_update", x.data_ptr(), x2.data_ptr(), xn.data_ptr(), nb, n,
+                  float(nocc), tol, done.data_ptr(), st)
+        x, xn = xn, x
+        if step % check_every == check_every - 1 and bool(done.all()):
             break
-        square = (tr2 - target).abs() < (2.0 * tr - tr2 - target).abs()
-        x = torch.where(square[:, None, None], x2, 2.0 * x - x2)
     return 0.5 * (x + x.transpose(1, 2))
 
 
-def occupied_factor(proj: torch.Tensor, guess: torch.Tensor) -> torch.Tensor:
-    """Orthonormal basis of range(proj) (rank = guess columns) by Cholesky-QR2 of proj @ guess."""
-    y = torch.bmm(proj, guess)
-    for _ in range(2):
-        g = torch.bmm(y.transpose(1, 2), y)
-        u, info = torch.linalg.cholesky_ex(g, upper=True)
-        if not bool((info == 0).all()):
-            raise FloatingPointError("occupied-space factorisation failed")
-        y = torch.linalg.solve_triangular(u, y, upper=True, left=False)
-    return y
+def occupied_factor(proj: torch.Tensor, guess: torch.Tensor, gen: torch.Generator) -> torch.Tensor:
+    """Orthonormal basis of range(proj) by Cholesky-QR2 of proj @ (guess + noise).
+
+    The previous occupied factor plus a random component keeps proj @ guess
+    full rank even when the occupied space rotates far between iterations;
+    a molecule whose factorisation still fails is retried with a purely random
+    start.
+    """
+    noise = torch.randn(guess.shape, dtype=guess.dtype, device=guess.device, generator=gen)
+    start = guess + 0.3 * noise
+    for attempt in range(2):
+        y = torch.bmm(proj, start)
+        ok = torch.ones(y.shape[0], dtype=torch.bool, device=y.device)
+        for _ in range(2):
+            g = torch.bmm(y.transpose(1, 2), y)
+            u, info = torch.linalg.cholesky_ex(g, upper=True)
+            ok &= info == 0
+            eye = torch.eye(g.shape[-1], dtype=g.dtype, device=g.device)
+            u = torch.where((info == 0)[:, None, None], u, eye)
+            y = torch.linalg.solve_triangular(u, y, upper=True, left=False)
+        if bool(ok.all()):
+            return y
+        start = torch.where(ok[:, None, None], start, noise)
+    raise FloatingPointError("occupied-space factorisation failed")
 
 
 def _diis_extrapolate(errs: list, focks: list) -> torch.Tensor:
@@ -242,8 +260,14 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
     with TIMER.stage("metric_factor"):
         mf = factor_metric(ints.metric, relative_threshold)
     with TIMER.stage("whiten"):
-        b_packed = torch.bmm(ints.a_packed, mf.inv_sqrt)  # (nb, P, X) whitened, FP64
+        b_packed = ints.a_packed  # whitened in place: B = A W, row blocks
         ints.a_packed = None  # the raw tensor is not needed after whitening
+        p_rows = b_packed.shape[1]
+        blk = max(1024, (1 << 27) // (8 * x))  # ~128 MB temporaries
+        for m in range(nb):
+            for r0 in range(0, p_rows, blk):
+                rows = b_packed[m, r0:r0 + blk]
+                rows.copy_(rows @ mf.inv_sqrt[m])
         jk = jkmod.make_builder(precision, b_packed, n, x, nocc)
         del b_packed
     s, h = ints.s, ints.h
@@ -267,7 +291,7 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
     def density_from(f, guess):
         with TIMER.stage("purify"):
             proj = purify_sp2(xo.transpose(1, 2) @ f @ xo, nocc)
-            co = occupied_factor(proj, guess)  # orthonormal, orthogonal basis
+            co = occupied_factor(proj, guess, gen)  # orthonormal, orthogonal basis
         return 2.0 * (xo @ proj @ xo.transpose(1, 2)), co
 
     d, co = density_from(h, guess)
