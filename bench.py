@@ -160,7 +160,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         return float(t.item())
 
     for _ in range(args.warmup):
-        batch.execute_device(xyz)
+        outs = batch.execute_device(xyz)
+        del outs
     torch.cuda.synchronize()
 
     # device-resident throughput
@@ -174,6 +175,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         start.record()
         for _ in range(args.steps):
             outs = batch.execute_device(xyz)
+            del outs
         end.record()
         torch.cuda.synchronize()
     barrier()
@@ -233,7 +235,6 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         "roofline": rl,
         "stages_ms_per_step": {k: round(v["ms"] / steps, 3) for k, v in stages.items()},
     }
-    del outs
     batch.close()
     return out
 

@@ -255,7 +255,16 @@ class PreparedBatch:
                       diis_history=calc.diis_history,
                       relative_threshold=calc.relative_threshold)
         grad = df_rhf_gradient(chunk, ints, out, xyz) if want_forces else None
-        return out, grad
+        # keep only per-molecule results; the chunk's B tensor and factors go
+        mf = out.pop("metric")
+        slim = {k: out[k] for k in ("energy", "converged", "iterations", "energy_change",
+                                    "density_rms", "density")}
+        slim["metric_rank"] = mf.rank
+        slim["metric_condition"] = mf.condition
+        slim["metric_kind"] = mf.kind
+        out.clear()
+        del ints
+        return slim, grad
 
     def upload_coordinates(self, coordinates=None) -> list:
         """Per-chunk device coordinate tensors (Bohr) for :meth:`execute_device`."""
@@ -325,8 +334,9 @@ class PreparedBatch:
                         executed_backend="cuda",
                         bucket_id=bucket,
                         basis_metadata={"nao": chunk.nao, "naux": chunk.naux,
-                                        "metric_rank": int(out["metric"].rank[j]),
-                                        "metric_condition": float(out["metric"].condition[j])},
+                                        "metric_rank": int(out["metric_rank"][j]),
+                                        "metric_condition": float(out["metric_condition"][j]),
+                                        "metric_factor": out["metric_kind"]},
                         precision={"mode": calc.precision},
                     )
         result = BatchResult(tuple(items))
