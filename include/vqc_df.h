@@ -135,6 +135,35 @@ int vqc_grad1e(vqc_plan* plan, const double* xyz, const double* dens, const doub
 int vqc_sp2_update(const double* x, const double* x2, double* xout, int32_t nmol, int32_t n,
                    double nocc, double tol, int32_t* done, void* stream);
 
+/*
+ * Mixed-precision J/K over the FP32 whitened tensor stored aux-major per AO
+ * row: b_aux_major[mol][mu][Q][nu], row length ld_ao >= nao (ld_ao % 4 == 0,
+ * padding zero).  Replaces the FP64 packed/dense B of the reference's CUDA
+ * plan (src/scf/cuda/df_plan_setup.cpp:70,224).
+ *   vqc_unpack_aux_major: packed whitened FP64 rows -> b_aux_major (FP32).
+ *   vqc_tc_half_transform: U[mol][mu][Q][i] = sum_nu B[mu][Q][nu] C[nu][i]
+ *     (3xTF32 tcgen05, FP32 out, i < o_pad, o_pad % 16 == 0, <= 128) and
+ *     rho[mol][Q] += 2 sum_{mu,i} U C[mu][i]; ct = C^T [mol][nocc][ld_ao]
+ *     FP32, c_occ = C [mol][nao][nocc] FP64.  Reference
+ *     src/scf/cuda/df_occupied_exchange.cpp:251-257 (U = B C).
+ *   vqc_tc_gram: kout[mol] += U U^T over kdim = naux * o_pad (3xTF32, FP64
+ *     output); reference df_occupied_exchange.cpp:262-279 (K = w U^T U).
+ *   vqc_coulomb_fp32: J[mol][mu][nu] = sum_Q B[mu][Q][nu] rho[mol][Q] (FP64
+ *     accumulate); reference src/scf/cuda/df_coulomb.cpp:24.
+ * error: device int set non-zero when a bounded wait inside a tensor-core
+ * kernel expires (the kernel then stops early; the caller must treat the
+ * output as invalid).
+ */
+int vqc_unpack_aux_major(const double* b_packed, int32_t nmol, int32_t nao, int32_t naux,
+                         int32_t ld_ao, float* b_aux_major, void* stream);
+int vqc_tc_half_transform(const float* b_aux_major, int32_t nmol, int32_t nao, int32_t ld_ao,
+                          int32_t naux, const float* ct, const double* c_occ, int32_t nocc,
+                          int32_t o_pad, float* u, double* rho, int32_t* error, void* stream);
+int vqc_tc_gram(const float* u, int32_t nmol, int32_t nao, int32_t kdim, double* kout,
+                int32_t* error, void* stream);
+int vqc_coulomb_fp32(const float* b_aux_major, const double* rho, int32_t nmol, int32_t nao,
+                     int32_t ld_ao, int32_t naux, double* j, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,99 @@
+"""Tensor-core split-precision GEMMs and the FP32 Coulomb kernel vs FP64 torch.
+
+3xTF32 with round-to-nearest splitting carries ~2^-22 relative product error;
+the tolerances below (1e-6 of the largest magnitude) sit well above that and
+far below what a TF32-only (2^-11) or truncated split would give.
+"""
+
+import pytest
+import torch
+
+from vibeqc_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("nb,n,x,o", [(2, 40, 200, 12), (1, 96, 464, 20), (3, 50, 130, 33),
+                                      (1, 384, 300, 80), (2, 72, 520, 100)])
+def test_half_transform_and_gram(nb, n, x, o):
+    ld = (n + 3) // 4 * 4
+    o_pad = (o + 15) // 16 * 16
+    g = torch.Generator(device="cuda").manual_seed(7)
+    b = torch.zeros(nb, n, x, ld, dtype=torch.float32, device="cuda")
+    b[..., :n] = torch.randn(nb, n, x, n, generator=g, device="cuda")
+    c = torch.randn(nb, n, o, generator=g, device="cuda", dtype=torch.float64) / n**0.5
+    ct = torch.zeros(nb, o, ld, dtype=torch.float32, device="cuda")
+    ct[:, :, :n] = c.transpose(1, 2)
+    u = torch.full((nb, n, x, o_pad), float("nan"), dtype=torch.float32, device="cuda")
+    rho = torch.zeros(nb, x, dtype=torch.float64, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    _lib.call("vqc_tc_half_transform", b.data_ptr(), nb, n, ld, x, ct.data_ptr(),
+              c.contiguous().data_ptr(), o, o_pad, u.data_ptr(), rho.data_ptr(), err.data_ptr(), st)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    b64 = b[..., :n].double()
+    c32 = ct[:, :, :n].transpose(1, 2).double()  # the FP32 C the kernel multiplied
+    ref = torch.einsum("bmqn,bni->bmqi", b64, c32)
+    got = u[..., :o].double()
+    scale = ref.abs().max().item()
+    assert torch.isfinite(u).all()
+    assert (got - ref).abs().max().item() <= 1e-6 * scale
+    assert (u[..., o:] == 0).all()
+    ref_rho = 2.0 * torch.einsum("bmi,bmqi->bq", c, ref)
+    assert (rho - ref_rho).abs().max().item() <= 1e-6 * ref_rho.abs().max().item()
+
+    kdim = x * o_pad
+    k = torch.zeros(nb, n, n, dtype=torch.float64, device="cuda")
+    _lib.call("vqc_tc_gram", u.data_ptr(), nb, n, kdim, k.data_ptr(), err.data_ptr(), st)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    uf = u.reshape(nb, n, kdim).double()
+    kref = uf @ uf.transpose(1, 2)
+    assert (k - kref).abs().max().item() <= 1e-6 * kref.abs().max().item()
+
+
+@pytest.mark.parametrize("nb,n,x", [(2, 40, 200), (1, 384, 1856), (3, 13, 77)])
+def test_coulomb_fp32(nb, n, x):
+    ld = (n + 3) // 4 * 4
+    g = torch.Generator(device="cuda").manual_seed(3)
+    full = torch.randn(nb, n, n, x, generator=g, device="cuda", dtype=torch.float64)
+    full = 0.5 * (full + full.transpose(1, 2))
+    b = torch.zeros(nb, n, x, ld, dtype=torch.float32, device="cuda")
+    b[..., :n] = full.permute(0, 1, 3, 2).float()
+    rho = torch.randn(nb, x, generator=g, device="cuda", dtype=torch.float64)
+    j = torch.empty(nb, n, n, dtype=torch.float64, device="cuda")
+    _lib.call("vqc_coulomb_fp32", b.data_ptr(), rho.data_ptr(), nb, n, ld, x, j.data_ptr(),
+              torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    ref = torch.einsum("bmqn,bq->bmn", b[..., :n].double(), rho)
+    assert (j - ref).abs().max().item() <= 1e-12 * ref.abs().max().item() * x**0.5
+
+
+def test_unpack_aux_major_roundtrip():
+    nb, n, x = 2, 11, 37
+    ld = 12
+    p = n * (n + 1) // 2
+    g = torch.Generator(device="cuda").manual_seed(5)
+    bp = torch.randn(nb, p, x, generator=g, device="cuda", dtype=torch.float64)
+    b = torch.full((nb, n, x, ld), 7.0, dtype=torch.float32, device="cuda")
+    _lib.call("vqc_unpack_aux_major", bp.data_ptr(), nb, n, x, ld, b.data_ptr(),
+              torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    mu = torch.arange(n, device="cuda")
+    hi = torch.maximum(mu[:, None], mu[None, :])
+    lo = torch.minimum(mu[:, None], mu[None, :])
+    idx = (hi * (hi + 1) // 2 + lo)
+    ref = bp[:, idx, :].permute(0, 1, 3, 2).float()  # (nb, mu, Q, nu)
+    assert torch.equal(b[..., :n], ref)
+    assert (b[..., n:] == 0).all()
+
+
+def test_bad_arguments_rejected():
+    st = torch.cuda.current_stream().cuda_stream
+    with pytest.raises(_lib.VqcError):
+        _lib.call("vqc_tc_half_transform", 0, 1, 8, 8, 8, 0, 0, 4, 16, 0, 0, 0, st)
+    x = torch.zeros(64, dtype=torch.float32, device="cuda")
+    with pytest.raises(_lib.VqcError):  # o_pad above the supported tile
+        _lib.call("vqc_tc_half_transform", x.data_ptr(), 1, 8, 8, 8, x.data_ptr(), x.data_ptr(),
+                  140, 144, x.data_ptr(), x.data_ptr(), x.data_ptr(), st)

@@ -88,6 +88,15 @@ _SIGNATURES = {
     "vqc_grad1e": ([_P, _P, _P, _P, _P, _P], ctypes.c_int),
     "vqc_sp2_update": ([_P, _P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
                         ctypes.c_double, _P, _P], ctypes.c_int),
+    "vqc_unpack_aux_major": ([_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                              ctypes.c_int32, _P, _P], ctypes.c_int),
+    "vqc_tc_half_transform": ([_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                               ctypes.c_int32, _P, _P, ctypes.c_int32, ctypes.c_int32, _P, _P,
+                               _P, _P], ctypes.c_int),
+    "vqc_tc_gram": ([_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _P, _P, _P],
+                    ctypes.c_int),
+    "vqc_coulomb_fp32": ([_P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                          ctypes.c_int32, _P, _P], ctypes.c_int),
 }
 
 _lib = None

@@ -50,15 +50,13 @@ def df_rhf_gradient(chunk, ints, scf_out: dict, xyz: torch.Tensor) -> torch.Tens
 
     wctx = TIMER.stage("grad_weights")
     wctx.__enter__()
-    b = jk.whitened_fp64()  # (nb, N*N, X) whitened, FP64
+    rho_all, u_all = jk.half_transform(c)  # fitted density and U = B C (per builder precision)
     rows = _packed_rows(n, dev)
     abar = torch.empty(nb, rows.numel(), x, dtype=torch.float64, device=dev)
     mbar = torch.empty(nb, x, x, dtype=torch.float64, device=dev)
     for m in range(nb):  # per molecule: bounded temporaries
-        bm = b[m]
-        rho_w = dens[m].reshape(1, n * n) @ bm  # (1, X)
-        cvec = (mf.inv_sqrt[m] @ rho_w[0])  # raw-basis c = Minv rho
-        u = torch.matmul(bm.view(n, n, x).transpose(1, 2), c[m])  # (N(mu), X, o(j))
+        cvec = mf.inv_sqrt[m] @ rho_all[m]  # raw-basis c = Minv rho
+        u = u_all[m].to(torch.float64)  # (N(mu), X, o(j))
         bij = torch.einsum("mi,mqj->qij", c[m], u)  # (X, o, o)
         del u
         gam = (mf.inv_sqrt[m] @ bij.reshape(x, o * o)).view(x, o, o)

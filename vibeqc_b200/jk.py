@@ -4,6 +4,12 @@
 comparator the mixed path is measured against.  J = B (B^T d) as in
 ``src/scf/cuda/df_coulomb.cpp:24``; occupied-factor K = 2 sum_Q (B_Q C)(B_Q C)^T
 as in ``src/scf/cuda/df_occupied_exchange.cpp:191-300``.
+
+``mixed``: B stored once in FP32 (aux-major per AO row); the exchange half
+transform U = B C and the Gram product K = 2 U U^T run on the tcgen05 tensor
+cores in split precision (3xTF32: round-to-nearest hi/lo parts, FP32
+accumulation drained to FP64), the fitted density rho comes out of the half
+transform's epilogue, and J streams the FP32 B once with FP64 accumulation.
 """
 
 from __future__ import annotations
@@ -50,7 +56,84 @@ class FP64Builder:
         return self.b
 
 
+    def half_transform(self, c_occ: torch.Tensor):
+        """(rho_whitened (nb, X), U (nb, N, X, o)) for D = 2 C C^T."""
+        nb, n, x, o = c_occ.shape[0], self.n, self.x, self.nocc
+        b4 = self.b.view(nb, n, n, x)
+        u = torch.matmul(b4.transpose(2, 3), c_occ[:, None, :, :])  # (nb, N, X, o)
+        rho = 2.0 * torch.einsum("bmi,bmqi->bq", c_occ, u)
+        return rho, u
+
+
+def _round_up(v: int, m: int) -> int:
+    return (v + m - 1) // m * m
+
+
+class MixedBuilder:
+    """FP32 B (aux-major per AO row) with tcgen05 3xTF32 exchange."""
+
+    precision = "mixed"
+
+    def __init__(self, b_packed: torch.Tensor, n: int, x: int, nocc: int):
+        from . import _lib
+
+        self._lib = _lib
+        nb = b_packed.shape[0]
+        self.nb, self.n, self.x, self.nocc = nb, n, x, nocc
+        self.ld = _round_up(n, 4)
+        self.o_pad = _round_up(nocc, 16)
+        if self.o_pad > 128:
+            raise _lib.VqcError(1, "mixed exchange supports at most 128 occupied orbitals")
+        dev = b_packed.device
+        self.b = torch.empty(nb, n, x, self.ld, dtype=torch.float32, device=dev)
+        self.st = torch.cuda.current_stream().cuda_stream
+        _lib.call("vqc_unpack_aux_major", b_packed.contiguous().data_ptr(), nb, n, x, self.ld,
+                  self.b.data_ptr(), self.st)
+        self.u = torch.empty(nb, n, x, self.o_pad, dtype=torch.float32, device=dev)
+        self.rho = torch.empty(nb, x, dtype=torch.float64, device=dev)
+        self.err = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.nbuild = 0
+
+    def _check(self):
+        if int(self.err.item()) != 0:
+            raise self._lib.VqcError(6, f"tensor-core kernel wait expired (code {int(self.err.item())})")
+
+    def _half(self, c_occ: torch.Tensor):
+        nb, n, o = self.nb, self.n, self.nocc
+        ct = torch.zeros(nb, o, self.ld, dtype=torch.float32, device=c_occ.device)
+        ct[:, :, :n] = c_occ.transpose(1, 2)
+        c64 = c_occ.contiguous()
+        self.rho.zero_()
+        with TIMER.stage("K_half_tc"):
+            self._lib.call("vqc_tc_half_transform", self.b.data_ptr(), nb, n, self.ld, self.x,
+                           ct.data_ptr(), c64.data_ptr(), o, self.o_pad, self.u.data_ptr(),
+                           self.rho.data_ptr(), self.err.data_ptr(), self.st)
+
+    def build(self, d: torch.Tensor, c_occ: torch.Tensor):
+        nb, n = self.nb, self.n
+        self._half(c_occ)
+        j = torch.empty(nb, n, n, dtype=torch.float64, device=d.device)
+        with TIMER.stage("J_fp32"):
+            self._lib.call("vqc_coulomb_fp32", self.b.data_ptr(), self.rho.data_ptr(), nb, n,
+                           self.ld, self.x, j.data_ptr(), self.st)
+        k = torch.zeros(nb, n, n, dtype=torch.float64, device=d.device)
+        with TIMER.stage("K_gram_tc"):
+            self._lib.call("vqc_tc_gram", self.u.data_ptr(), nb, n, self.x * self.o_pad,
+                           k.data_ptr(), self.err.data_ptr(), self.st)
+        self.nbuild += 1
+        self._check()
+        return j, 2.0 * k
+
+    def half_transform(self, c_occ: torch.Tensor):
+        """(rho_whitened (nb, X), U (nb, N, X, o) as FP64) for D = 2 C C^T."""
+        self._half(c_occ)
+        self._check()
+        return self.rho.clone(), self.u[..., : self.nocc]
+
+
 def make_builder(precision: str, b_packed: torch.Tensor, n: int, x: int, nocc: int):
     if precision == "fp64":
         return FP64Builder(b_packed, n, x, nocc)
+    if precision == "mixed":
+        return MixedBuilder(b_packed, n, x, nocc)
     raise ValueError(f"unknown precision {precision!r}")
