@@ -34,7 +34,7 @@ namespace tc {
 constexpr int BM = 128;
 constexpr int BK = 32;  // FP32 elements per K-block: one 128-byte swizzle row
 constexpr int THREADS = 128;
-constexpr int kFlush = 8;  // K-blocks per FP32 accumulation chain in kGram
+constexpr int kFlush = 4;  // K-blocks per FP32 accumulation chain in kGram
 constexpr unsigned long long kWaitNs = 2000000000ull;
 
 enum Mode { kHalf = 0, kGram = 1 };

@@ -50,7 +50,10 @@ def df_rhf_gradient(chunk, ints, scf_out: dict, xyz: torch.Tensor) -> torch.Tens
 
     wctx = TIMER.stage("grad_weights")
     wctx.__enter__()
-    rho_all, u_all = jk.half_transform(c)  # fitted density and U = B C (per builder precision)
+    if scf_out.get("exact_half") is not None:
+        rho_all, u_all = scf_out["exact_half"]  # FP64 U = B C already formed for the energy
+    else:
+        rho_all, u_all = jk.half_transform(c)  # fitted density and U = B C
     rows = _packed_rows(n, dev)
     abar = torch.empty(nb, rows.numel(), x, dtype=torch.float64, device=dev)
     mbar = torch.empty(nb, x, x, dtype=torch.float64, device=dev)

@@ -125,10 +125,23 @@ class MixedBuilder:
         return j, 2.0 * k
 
     def half_transform(self, c_occ: torch.Tensor):
-        """(rho_whitened (nb, X), U (nb, N, X, o) as FP64) for D = 2 C C^T."""
-        self._half(c_occ)
-        self._check()
-        return self.rho.clone(), self.u[..., : self.nocc]
+        """FP64-arithmetic (rho_whitened (nb, X), U (nb, N, X, o)) over the FP32 B.
+
+        Used for the final energy and the gradient weights: the operands are
+        the stored FP32 B upcast per molecule, so the only deviation from the
+        FP64 path is the FP32 storage rounding of B.
+        """
+        nb, n, x, o = self.nb, self.n, self.x, self.nocc
+        dev = c_occ.device
+        u = torch.empty(nb, n, x, o, dtype=torch.float64, device=dev)
+        rho = torch.empty(nb, x, dtype=torch.float64, device=dev)
+        with TIMER.stage("exact_half_fp64"):
+            for m in range(nb):
+                bm = self.b[m, :, :, :n].to(torch.float64)  # (mu, Q, nu)
+                u[m] = torch.matmul(bm, c_occ[m])  # (mu, Q, i)
+                del bm
+                rho[m] = 2.0 * torch.einsum("mi,mqi->q", c_occ[m], u[m])
+        return rho, u
 
 
 def make_builder(precision: str, b_packed: torch.Tensor, n: int, x: int, nocc: int):

@@ -144,6 +144,19 @@ def factor_metric(metric: torch.Tensor, relative_threshold: float = 1e-10) -> Me
     return MetricFactor(lam, vec, keep, inv_sqrt, rank, cond, "eigen")
 
 
+def exact_energy(jk, d: torch.Tensor, c: torch.Tensor, h: torch.Tensor,
+                 enuc: torch.Tensor) -> torch.Tensor:
+    """E = tr(D H) + |rho|^2 / 2 - sum_{Q,i,j} (C^T B_Q C)_{ij}^2 + E_nn in FP64 arithmetic."""
+    rho, u = jk.half_transform(c)
+    e1 = torch.einsum("bmn,bmn->b", d, h)
+    ej = 0.5 * (rho * rho).sum(dim=1)
+    ek = torch.zeros_like(ej)
+    for m in range(d.shape[0]):
+        bij = torch.einsum("mi,mqj->qij", c[m], u[m])
+        ek[m] = -(bij * bij).sum()
+    return e1 + ej + ek + enuc, (rho, u)
+
+
 class Chunk:
     """A homogeneous group of molecules sharing one native plan."""
 
@@ -308,6 +321,12 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
     f_final = torch.zeros_like(d)
     errs, focks = [], []
     comm_tol = 10.0 * min(1e-8, density_tolerance)
+    if jk.precision == "mixed":
+        # the tensor-core operators carry ~1e-6 relative error: converge the
+        # iterations to that floor; the energy is re-evaluated in FP64 below
+        energy_tolerance = max(energy_tolerance, 1e-8)
+        density_tolerance = max(density_tolerance, 1e-7)
+        comm_tol = max(comm_tol, 1e-6)
     for it in range(1, max_iterations + 1):
         j, k = jk.build(d, c)
         TIMER_ctx = TIMER.stage("scf_other")
@@ -349,9 +368,17 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
         d = torch.where(active[:, None, None], d_new, d)
         c = torch.where(active[:, None, None], c_new, c)
         TIMER_ctx.__exit__(None, None, None)
+    if jk.precision == "mixed":
+        # final energy in FP64 arithmetic at the converged density: the SCF
+        # operators above carry the tensor cores' accumulation error, the
+        # energy is variational in D, so re-evaluating E[D] removes it to
+        # second order (the FP32 storage of B remains)
+        final_e, exact_half = exact_energy(jk, d_final, c_final, h, enuc)
+    else:
+        exact_half = None
     return {
         "energy": final_e, "converged": converged, "iterations": iters,
         "energy_change": final_de, "density_rms": final_drms, "density": d_final,
-        "orbitals": c_final, "fock": f_final,
+        "orbitals": c_final, "fock": f_final, "exact_half": exact_half,
         "metric": mf, "orthogonalizer": xo, "enuc": enuc, "charges": zs, "jk": jk,
     }
