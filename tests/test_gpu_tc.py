@@ -1,12 +1,12 @@
 """Tensor-core split-precision GEMMs and the FP32 Coulomb kernel vs FP64 torch.
 
-3xTF32 with round-to-nearest splitting carries ~2^-22 relative product error;
-the half transform is checked at 1e-6 of the largest magnitude.  The Gram
-product sums long chains of same-sign terms, where the tensor core's FP32
-accumulation (not round-to-nearest) leaves a coherent relative bias of about
-2^-24 per accumulation step; with the accumulator drained to FP64 every
-kFlush K-blocks the diagonal stays within 5e-6 relative, which the test pins.
-A TF32-only product (2^-11) would miss both bounds by orders of magnitude.
+3xTF32 with round-to-nearest splitting carries ~2^-22 relative product error,
+but the tensor core's FP32 accumulation is not round-to-nearest: it leaves a
+relative bias of about 2^-24 per accumulation step along a chain, so a chain
+of L steps is good to ~L * 2^-25.  The half transform (L <= 144 for N <= 384)
+and the Gram product (accumulator drained to FP64 every kFlush K-blocks) both
+stay within 5e-6 relative, which the tests pin.  A TF32-only product (2^-11)
+would miss that bound by orders of magnitude.
 """
 
 import pytest
@@ -42,7 +42,7 @@ def test_half_transform_and_gram(nb, n, x, o):
     got = u[..., :o].double()
     scale = ref.abs().max().item()
     assert torch.isfinite(u).all()
-    assert (got - ref).abs().max().item() <= 1e-6 * scale
+    assert (got - ref).abs().max().item() <= 5e-6 * scale
     assert (u[..., o:] == 0).all()
     ref_rho = 2.0 * torch.einsum("bmi,bmqi->bq", c, ref)
     assert (rho - ref_rho).abs().max().item() <= 1e-6 * ref_rho.abs().max().item()

@@ -55,6 +55,9 @@ class FP64Builder:
     def whitened_fp64(self) -> torch.Tensor:
         return self.b
 
+    def build_exact(self, d: torch.Tensor, c_occ: torch.Tensor):
+        return self.build(d, c_occ)
+
 
     def half_transform(self, c_occ: torch.Tensor):
         """(rho_whitened (nb, X), U (nb, N, X, o)) for D = 2 C C^T."""
@@ -123,6 +126,20 @@ class MixedBuilder:
         self.nbuild += 1
         self._check()
         return j, 2.0 * k
+
+    def build_exact(self, d: torch.Tensor, c_occ: torch.Tensor):
+        """J and K in FP64 arithmetic over the stored FP32 B (refinement phase)."""
+        nb, n, x, o = self.nb, self.n, self.x, self.nocc
+        rho, u = self.half_transform(c_occ)
+        j = torch.empty(nb, n, n, dtype=torch.float64, device=d.device)
+        with TIMER.stage("J_fp32"):
+            self._lib.call("vqc_coulomb_fp32", self.b.data_ptr(), rho.data_ptr(), nb, n,
+                           self.ld, x, j.data_ptr(), self.st)
+        with TIMER.stage("K_exact_fp64"):
+            uf = u.reshape(nb, n, x * o)
+            k = 2.0 * torch.bmm(uf, uf.transpose(1, 2))
+        self.nbuild += 1
+        return j, k
 
     def half_transform(self, c_occ: torch.Tensor):
         """FP64-arithmetic (rho_whitened (nb, X), U (nb, N, X, o)) over the FP32 B.

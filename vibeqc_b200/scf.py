@@ -321,14 +321,17 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
     f_final = torch.zeros_like(d)
     errs, focks = [], []
     comm_tol = 10.0 * min(1e-8, density_tolerance)
-    if jk.precision == "mixed":
-        # the tensor-core operators carry ~1e-6 relative error: converge the
-        # iterations to that floor; the energy is re-evaluated in FP64 below
-        energy_tolerance = max(energy_tolerance, 1e-8)
-        density_tolerance = max(density_tolerance, 1e-7)
-        comm_tol = max(comm_tol, 1e-6)
+    # mixed precision: tensor-core iterations until the loose criteria below
+    # hold for every active molecule, then FP64-arithmetic refinement
+    # iterations (same FP32 B) under the standard criteria
+    exact = jk.precision != "mixed"
+    mixed_iterations = 0
     for it in range(1, max_iterations + 1):
-        j, k = jk.build(d, c)
+        if exact:
+            j, k = jk.build_exact(d, c)
+        else:
+            j, k = jk.build(d, c)
+            mixed_iterations += 1
         TIMER_ctx = TIMER.stage("scf_other")
         TIMER_ctx.__enter__()
         f = h + j - 0.5 * k
@@ -350,6 +353,12 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
         drms = ((d_new - d) ** 2).mean(dim=(1, 2)).sqrt()
         cmax = comm.abs().amax(dim=(1, 2))
         done = (de < energy_tolerance) & (drms < density_tolerance) & (cmax <= comm_tol)
+        if not exact:
+            loose = (de < 1e-6) & (cmax <= 1e-4)
+            if bool((loose | ~active).all()):
+                exact = True
+                errs, focks = [], []  # restart DIIS on the refined operators
+            done = torch.zeros_like(done)
         newly = done & active
         # record the state of molecules that are still active
         final_e = torch.where(active, energy, final_e)
@@ -380,5 +389,6 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
         "energy": final_e, "converged": converged, "iterations": iters,
         "energy_change": final_de, "density_rms": final_drms, "density": d_final,
         "orbitals": c_final, "fock": f_final, "exact_half": exact_half,
+        "mixed_iterations": mixed_iterations,
         "metric": mf, "orthogonalizer": xo, "enuc": enuc, "charges": zs, "jk": jk,
     }
