@@ -211,6 +211,19 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
               "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": round(ach / peaks["hbm_gbs"], 4),
               "traffic": None, "peak_source": peaks["source"],
               "note": "compute-bound FP64 Rys kernel; bytes are the FP64 tensor it writes"}
+    if "K_gram_tc" in stages:
+        peaks = _peaks()
+        builds = stages["K_gram_tc"]["launch_groups"] / steps  # one launch group per chunk build
+        t_gram = stages["K_gram_tc"]["ms"] / 1000.0 / steps
+        t_half = stages["K_half_tc"]["ms"] / 1000.0 / steps
+        nchunks = len(batch._chunks)
+        kflops = model["k_flops_per_build"] * builds / max(nchunks, 1)
+        ach = kflops / (t_gram + t_half) / 1e12
+        rl = {"kernel": "tcgen05 3xTF32 exchange (half transform + Gram)", "bound": "tensor",
+              "achieved": round(ach, 2), "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
+              "frac": round(ach / peaks["bf16_tflops"], 5), "traffic": None,
+              "peak_source": peaks["source"] + " (dense bf16 cuBLAS; algorithmic flops counted once, "
+                             "not x3 for the split products)"}
     out = {
         "metric": METRIC,
         "value": round(value, 3),

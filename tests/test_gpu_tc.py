@@ -45,7 +45,7 @@ def test_half_transform_and_gram(nb, n, x, o):
     assert (got - ref).abs().max().item() <= 5e-6 * scale
     assert (u[..., o:] == 0).all()
     ref_rho = 2.0 * torch.einsum("bmi,bmqi->bq", c, ref)
-    assert (rho - ref_rho).abs().max().item() <= 1e-6 * ref_rho.abs().max().item()
+    assert (rho - ref_rho).abs().max().item() <= 5e-6 * ref_rho.abs().max().item()
 
     kdim = x * o_pad
     k = torch.zeros(nb, n, n, dtype=torch.float64, device="cuda")

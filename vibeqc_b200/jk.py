@@ -94,6 +94,10 @@ class MixedBuilder:
                   self.b.data_ptr(), self.st)
         self.u = torch.empty(nb, n, x, self.o_pad, dtype=torch.float32, device=dev)
         self.rho = torch.empty(nb, x, dtype=torch.float64, device=dev)
+        # the FP64 whitened rows stay resident for the refinement iterations,
+        # the final energy and the gradient
+        self.b_packed = b_packed
+        self.idx = unpack_index(n, dev)
         self.err = torch.zeros(1, dtype=torch.int32, device=dev)
         self.nbuild = 0
 
@@ -128,25 +132,29 @@ class MixedBuilder:
         return j, 2.0 * k
 
     def build_exact(self, d: torch.Tensor, c_occ: torch.Tensor):
-        """J and K in FP64 arithmetic over the stored FP32 B (refinement phase)."""
+        """FP64 J and K from the FP64 whitened tensor (refinement phase)."""
         nb, n, x, o = self.nb, self.n, self.x, self.nocc
         rho, u = self.half_transform(c_occ)
-        j = torch.empty(nb, n, n, dtype=torch.float64, device=d.device)
-        with TIMER.stage("J_fp32"):
-            self._lib.call("vqc_coulomb_fp32", self.b.data_ptr(), rho.data_ptr(), nb, n,
-                           self.ld, x, j.data_ptr(), self.st)
+        with TIMER.stage("J_exact_fp64"):
+            j = torch.empty(nb, n, n, dtype=torch.float64, device=d.device)
+            for m in range(nb):
+                j[m] = (self._full64(m) @ rho[m]).view(n, n)
         with TIMER.stage("K_exact_fp64"):
             uf = u.reshape(nb, n, x * o)
             k = 2.0 * torch.bmm(uf, uf.transpose(1, 2))
         self.nbuild += 1
         return j, k
 
-    def half_transform(self, c_occ: torch.Tensor):
-        """FP64-arithmetic (rho_whitened (nb, X), U (nb, N, X, o)) over the FP32 B.
+    def _full64(self, m: int) -> torch.Tensor:
+        """(N*N, X) FP64 whitened rows of molecule m, unpacked on the fly."""
+        return self.b_packed[m][self.idx]
 
-        Used for the final energy and the gradient weights: the operands are
-        the stored FP32 B upcast per molecule, so the only deviation from the
-        FP64 path is the FP32 storage rounding of B.
+    def half_transform(self, c_occ: torch.Tensor):
+        """FP64 (rho_whitened (nb, X), U (nb, N, X, o)) from the FP64 whitened tensor.
+
+        Used by the refinement iterations, the final energy and the gradient
+        weights, so the reported energy and forces carry no FP32 storage or
+        tensor-core error.
         """
         nb, n, x, o = self.nb, self.n, self.x, self.nocc
         dev = c_occ.device
@@ -154,9 +162,9 @@ class MixedBuilder:
         rho = torch.empty(nb, x, dtype=torch.float64, device=dev)
         with TIMER.stage("exact_half_fp64"):
             for m in range(nb):
-                bm = self.b[m, :, :, :n].to(torch.float64)  # (mu, Q, nu)
-                u[m] = torch.matmul(bm, c_occ[m])  # (mu, Q, i)
-                del bm
+                b4 = self._full64(m).view(n, n, x)
+                u[m] = torch.matmul(b4.transpose(1, 2), c_occ[m])  # (mu, Q, i)
+                del b4
                 rho[m] = 2.0 * torch.einsum("mi,mqi->q", c_occ[m], u[m])
         return rho, u
 

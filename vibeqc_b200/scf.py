@@ -144,6 +144,9 @@ def factor_metric(metric: torch.Tensor, relative_threshold: float = 1e-10) -> Me
     return MetricFactor(lam, vec, keep, inv_sqrt, rank, cond, "eigen")
 
 
+MIXED_ITERATION_CAP = 24  # tensor-core iterations before refinement is forced
+
+
 def exact_energy(jk, d: torch.Tensor, c: torch.Tensor, h: torch.Tensor,
                  enuc: torch.Tensor) -> torch.Tensor:
     """E = tr(D H) + |rho|^2 / 2 - sum_{Q,i,j} (C^T B_Q C)_{ij}^2 + E_nn in FP64 arithmetic."""
@@ -355,7 +358,7 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
         done = (de < energy_tolerance) & (drms < density_tolerance) & (cmax <= comm_tol)
         if not exact:
             loose = (de < 1e-6) & (cmax <= 1e-4)
-            if bool((loose | ~active).all()):
+            if bool((loose | ~active).all()) or mixed_iterations >= MIXED_ITERATION_CAP:
                 exact = True
                 errs, focks = [], []  # restart DIIS on the refined operators
             done = torch.zeros_like(done)
