@@ -28,20 +28,28 @@ def test_half_transform_and_gram(nb, n, x, o):
     c = torch.randn(nb, n, o, generator=g, device="cuda", dtype=torch.float64) / n**0.5
     ct = torch.zeros(nb, o, ld, dtype=torch.float32, device="cuda")
     ct[:, :, :n] = c.transpose(1, 2)
-    u = torch.full((nb, n, x, o_pad), float("nan"), dtype=torch.float32, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    ct_hi, ct_lo = torch.empty_like(ct), torch.empty_like(ct)
+    _lib.call("vqc_split_tf32", ct.data_ptr(), ct_hi.data_ptr(), ct_lo.data_ptr(), ct.numel(), st)
+    u_hi = torch.full((nb, n, x, o_pad), float("nan"), dtype=torch.float32, device="cuda")
+    u_lo = torch.full_like(u_hi, float("nan"))
     rho = torch.zeros(nb, x, dtype=torch.float64, device="cuda")
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
-    st = torch.cuda.current_stream().cuda_stream
-    _lib.call("vqc_tc_half_transform", b.data_ptr(), nb, n, ld, x, ct.data_ptr(),
-              c.contiguous().data_ptr(), o, o_pad, u.data_ptr(), rho.data_ptr(), err.data_ptr(), st)
+    _lib.call("vqc_tc_half_transform", b.data_ptr(), nb, n, ld, x, ct_hi.data_ptr(),
+              ct_lo.data_ptr(), c.contiguous().data_ptr(), o, o_pad, u_hi.data_ptr(),
+              u_lo.data_ptr(), rho.data_ptr(), err.data_ptr(), st)
     torch.cuda.synchronize()
     assert int(err.item()) == 0
+    assert torch.isfinite(u_hi).all() and torch.isfinite(u_lo).all()
+    # the split parts are TF32-representable (low 13 mantissa bits clear)
+    assert ((u_hi.view(torch.int32) & 0x1FFF) == 0).all()
+    assert ((u_lo.view(torch.int32) & 0x1FFF) == 0).all()
     b64 = b[..., :n].double()
-    c32 = ct[:, :, :n].transpose(1, 2).double()  # the FP32 C the kernel multiplied
-    ref = torch.einsum("bmqn,bni->bmqi", b64, c32)
-    got = u[..., :o].double()
+    c_used = (ct_hi + ct_lo)[:, :, :n].transpose(1, 2).double()  # the C the kernel multiplied
+    ref = torch.einsum("bmqn,bni->bmqi", b64, c_used)
+    u = u_hi.double() + u_lo.double()
+    got = u[..., :o]
     scale = ref.abs().max().item()
-    assert torch.isfinite(u).all()
     assert (got - ref).abs().max().item() <= 5e-6 * scale
     assert (u[..., o:] == 0).all()
     ref_rho = 2.0 * torch.einsum("bmi,bmqi->bq", c, ref)
@@ -49,12 +57,25 @@ def test_half_transform_and_gram(nb, n, x, o):
 
     kdim = x * o_pad
     k = torch.zeros(nb, n, n, dtype=torch.float64, device="cuda")
-    _lib.call("vqc_tc_gram", u.data_ptr(), nb, n, kdim, k.data_ptr(), err.data_ptr(), st)
+    _lib.call("vqc_tc_gram", u_hi.data_ptr(), u_lo.data_ptr(), nb, n, kdim, k.data_ptr(),
+              err.data_ptr(), st)
     torch.cuda.synchronize()
     assert int(err.item()) == 0
-    uf = u.reshape(nb, n, kdim).double()
+    uf = u.reshape(nb, n, kdim)
     kref = uf @ uf.transpose(1, 2)
     assert (k - kref).abs().max().item() <= 5e-6 * kref.abs().max().item()
+    assert torch.equal(k, k.transpose(1, 2)) or (k - k.transpose(1, 2)).abs().max() <= 1e-12 * kref.abs().max()
+
+
+def test_split_tf32_exact_sum():
+    x = torch.randn(10007, device="cuda", dtype=torch.float32) * 1e3
+    hi, lo = torch.empty_like(x), torch.empty_like(x)
+    _lib.call("vqc_split_tf32", x.data_ptr(), hi.data_ptr(), lo.data_ptr(), x.numel(),
+              torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert ((hi.view(torch.int32) & 0x1FFF) == 0).all()
+    err = (hi.double() + lo.double() - x.double()).abs() / x.double().abs().clamp_min(1e-30)
+    assert err.max().item() <= 2.0**-21
 
 
 @pytest.mark.parametrize("nb,n,x", [(2, 40, 200), (1, 384, 1856), (3, 13, 77)])
@@ -96,8 +117,8 @@ def test_unpack_aux_major_roundtrip():
 def test_bad_arguments_rejected():
     st = torch.cuda.current_stream().cuda_stream
     with pytest.raises(_lib.VqcError):
-        _lib.call("vqc_tc_half_transform", 0, 1, 8, 8, 8, 0, 0, 4, 16, 0, 0, 0, st)
+        _lib.call("vqc_tc_half_transform", 0, 1, 8, 8, 8, 0, 0, 0, 4, 16, 0, 0, 0, 0, st)
     x = torch.zeros(64, dtype=torch.float32, device="cuda")
     with pytest.raises(_lib.VqcError):  # o_pad above the supported tile
         _lib.call("vqc_tc_half_transform", x.data_ptr(), 1, 8, 8, 8, x.data_ptr(), x.data_ptr(),
-                  140, 144, x.data_ptr(), x.data_ptr(), x.data_ptr(), st)
+                  x.data_ptr(), 140, 144, x.data_ptr(), x.data_ptr(), x.data_ptr(), x.data_ptr(), st)

@@ -1,27 +1,33 @@
 // Split-precision (3xTF32) tensor-core GEMMs for the mixed-precision exchange.
 //
-// D[M x N] = A[M x K] . B[N x K]^T with FP32 operands in HBM (both K-major),
-// computed on the 5th-generation tensor cores as
-//     D = A_hi B_hi^T + A_hi B_lo^T + A_lo B_hi^T,
+// Products are formed on the 5th-generation tensor cores (tcgen05.mma
+// kind::tf32, M = 128, accumulator in TMEM) as
+//     A B^T = A_hi B_hi^T + A_hi B_lo^T + A_lo B_hi^T,
 // x_hi = rn_tf32(x), x_lo = rn_tf32(x - x_hi): round-to-nearest splitting, so
 // the products carry ~2^-22 relative error without the one-sided bias of
-// truncation.  Operand tiles arrive by TMA (128-byte swizzle) into shared
-// memory; all 128 threads split them in place (hi) and into a sibling buffer
-// (lo); one thread issues tcgen05.mma (kind::tf32, M = 128) into a TMEM
-// accumulator and commits to an mbarrier that releases the stage.
+// truncation.  Operand tiles arrive by TMA (128-byte swizzle, K-major).
 //
-// Two epilogues:
-//   kHalf  -- U = B_mu^T C (the exchange half transform, K = N_ao): FP32 store
-//             of U and rho[Q] += 2 sum_i U[Q][i] C[mu][i] (the fitted density
-//             that J needs), reference src/scf/cuda/df_occupied_exchange.cpp:251
-//   kGram  -- K += U U^T over K = X * o (reference df_occupied_exchange.cpp:262):
-//             the FP32 TMEM accumulator is drained into FP64 registers every
-//             kFlush K-blocks, bounding the FP32 accumulation chain; partial
-//             tiles of a split K range are added into FP64 output.
+//   half_ws_kernel -- U[mol][mu][Q][i] = sum_nu B[mol][mu][Q][nu] C[nu][i]
+//     (reference src/scf/cuda/df_occupied_exchange.cpp:251-257).  Persistent
+//     over (mu, 128-row Q tile) items.  Warp roles: one TMA producer, four
+//     splitter warps that split the streamed FP32 B tile (hi in place, lo in a
+//     sibling buffer), one MMA-issuing thread, four epilogue warps.  C arrives
+//     pre-split.  Two TMEM accumulators let an item's epilogue (U written
+//     already split, rho[Q] += 2 sum_i U C[mu][i] for J) overlap the next
+//     item's MMAs.  The kernel streams B once: HBM-bound by design.
+//   gram_ws_kernel -- K[mol] += U U^T over kdim = X * o_pad (reference
+//     df_occupied_exchange.cpp:262-279) from the pre-split U: a pure
+//     TMA -> MMA pipeline over upper-triangle 128x128 tiles and split K
+//     ranges.  The tensor core's FP32 accumulation is not round-to-nearest
+//     (about 2^-24 relative bias per accumulation step), so chains are kept to
+//     kGramFlush K-blocks and drained into FP64 registers by eight epilogue
+//     warps (double-buffered TMEM); tiles add FP64 partials (and the mirror
+//     of off-diagonal tiles) into the output.
 //
 // Every mbarrier wait is bounded by a 2 s %globaltimer budget; on expiry the
-// CTA records an error code, stops issuing work, waits (bounded) for its own
-// copies and MMAs in flight, frees its TMEM and returns.
+// CTA records an error code, every role stops issuing work, thread 0 waits
+// (bounded) for the copies and MMAs it has in flight, TMEM is freed and the
+// kernel returns.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -33,36 +39,7 @@ namespace tc {
 
 constexpr int BM = 128;
 constexpr int BK = 32;  // FP32 elements per K-block: one 128-byte swizzle row
-constexpr int THREADS = 128;
-constexpr int kFlush = 4;  // K-blocks per FP32 accumulation chain in kGram
 constexpr unsigned long long kWaitNs = 2000000000ull;
-
-enum Mode { kHalf = 0, kGram = 1 };
-
-struct Params {
-  int m, n, kdim;
-  int kblocks_per_split, ksplit;
-  int b_batch_div;
-  float* u;          // kHalf: [z][m][ldu]
-  int ldu;
-  double* rho;       // kHalf: [z / rho_div][m]
-  const double* cvec;  // kHalf: [z][cld]
-  int cld, ncvec, rho_div;
-  double* kout;      // kGram: [z][m][n]
-  int* error;
-};
-
-template <int BN>
-struct Cfg {
-  static constexpr int A_BYTES = BM * BK * 4;
-  static constexpr int B_BYTES = BN * BK * 4;
-  static constexpr int STAGE = 2 * A_BYTES + 2 * B_BYTES;
-  static constexpr int STAGES = (220 * 1024) / STAGE >= 4 ? 4 : (220 * 1024) / STAGE;
-  static constexpr int SMEM = STAGES * STAGE + 1024 + 256;
-  static constexpr int TMEM_COLS = BN <= 32 ? 32 : (BN <= 64 ? 64 : (BN <= 128 ? 128 : 256));
-  static_assert(BN % 16 == 0 && BN >= 16 && BN <= 256, "M=128 tf32 MMA needs N % 16 == 0");
-  static_assert(STAGES >= 2, "shared memory too small for the pipeline");
-};
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -174,226 +151,454 @@ __device__ __forceinline__ void split4(float4& v, float4& lo) {
   h = rn_tf32(v.w); lo.w = rn_tf32(v.w - h); v.w = h;
 }
 
-template <int BN, int MODE>
-__global__ void __launch_bounds__(THREADS, 1)
-    tf32x3_gemm_kernel(const __grid_constant__ CUtensorMap tmA,
-                       const __grid_constant__ CUtensorMap tmB, Params p) {
-  using C = Cfg<BN>;
-  constexpr int S = C::STAGES;
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// Shared control block behind the operand stages.
+struct Ctrl {
+  uint64_t full[4], conv[4], empty[4], acc_full[2], acc_empty[2];
+  uint32_t tmem;
+  int abort;
+  int issued;    // k-steps the producer issued
+  int consumed;  // k-steps whose operands have been taken over (full barrier passed)
+  int commits;   // MMA commits to empty barriers
+};
+
+__device__ __forceinline__ void set_abort(Ctrl* c, int* error, int code) {
+  if (error) atomicExch(error, code);
+  *reinterpret_cast<volatile int*>(&c->abort) = 1;
+}
+
+__device__ __forceinline__ bool aborted(Ctrl* c) {
+  return *reinterpret_cast<volatile int*>(&c->abort) != 0;
+}
+
+// ---------------------------------------------------------------------------
+// half transform: U[z][Q][i] = sum_nu B[z][Q][nu] C[mol(z)][i][nu], 3xTF32,
+// persistent over (z, 128-row Q tile) items; warp roles:
+//   w0 TMA producer, w1-w4 splitters (A -> hi in place + lo), w5 MMA issuer,
+//   w6-w9 epilogue (TMEM -> U hi/lo in HBM, rho partial sums)
+// ---------------------------------------------------------------------------
+
+constexpr int kHalfThreads = 320;
+constexpr int kGramThreads = 320;
+constexpr int kTmemBuf = 128;  // columns per accumulator buffer (two buffers)
+
+template <int BN>
+struct HalfCfg {
+  static constexpr int A_BYTES = BM * BK * 4;
+  static constexpr int C_BYTES = BN * BK * 4;
+  static constexpr int STAGE = 2 * A_BYTES + 2 * C_BYTES;
+  static constexpr int S = (214 * 1024) / STAGE >= 4 ? 4 : (214 * 1024) / STAGE;
+  static constexpr int SMEM = S * STAGE + 1024 + (int)sizeof(Ctrl) + 64;
+  static_assert(BN % 16 == 0 && BN >= 16 && BN <= kTmemBuf, "BN");
+  static_assert(S >= 2, "pipeline");
+};
+
+struct HalfParams {
+  int nao, naux, nocc, ldu, nitems, nqt, nk;
+  float* u_hi;
+  float* u_lo;
+  double* rho;
+  const double* cvec;
+  int* error;
+};
+
+template <int BN>
+__global__ void __launch_bounds__(kHalfThreads, 1)
+    half_ws_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmCh,
+                   const __grid_constant__ CUtensorMap tmCl, HalfParams p) {
+  using C = HalfCfg<BN>;
+  constexpr int S = C::S;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + S * C::STAGE);
-  // bars[0..S): full, bars[S..2S): empty, bars[2S]: accumulator ready
-  volatile uint32_t* tmem_slot = reinterpret_cast<volatile uint32_t*>(bars + 2 * S + 1);
-  volatile int* abort = reinterpret_cast<volatile int*>(bars + 2 * S + 2);
-
-  const int tid = threadIdx.x;
-  const int warp = tid >> 5;
-  const int z = blockIdx.z / p.ksplit, split = blockIdx.z % p.ksplit;
-  const int zb = z / p.b_batch_div;
-  const int row0 = blockIdx.x * BM, col0 = blockIdx.y * BN;
-  const int kb_total = (p.kdim + BK - 1) / BK;
-  const int kb0 = split * p.kblocks_per_split;
-  const int kb1 = min(kb_total, kb0 + p.kblocks_per_split);
-  const int nkb = kb1 - kb0;
-  if (nkb <= 0) return;  // uniform per CTA
-
-  const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + S), accb = smem_u32(bars + 2 * S);
+  Ctrl* ctrl = reinterpret_cast<Ctrl*>(smem + S * C::STAGE);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t full0 = smem_u32(ctrl->full), conv0 = smem_u32(ctrl->conv);
+  const uint32_t empty0 = smem_u32(ctrl->empty), af0 = smem_u32(ctrl->acc_full);
+  const uint32_t ae0 = smem_u32(ctrl->acc_empty);
   if (tid == 0) {
     for (int s = 0; s < S; ++s) {
       mbar_init(full0 + 8 * s, 1);
+      mbar_init(conv0 + 8 * s, 4);
       mbar_init(empty0 + 8 * s, 1);
     }
-    mbar_init(accb, 1);
-    *abort = 0;
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(af0 + 8 * b, 1);
+      mbar_init(ae0 + 8 * b, 4);
+    }
+    ctrl->abort = 0;
+    ctrl->issued = ctrl->consumed = ctrl->commits = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                     smem_u32(const_cast<uint32_t*>(tmem_slot))),
-                 "r"(C::TMEM_COLS)
+                     smem_u32(&ctrl->tmem)),
+                 "r"(2 * kTmemBuf)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   fence_before_sync();
   __syncthreads();
   fence_after_sync();
-  const uint32_t tmem = *tmem_slot;
-  constexpr uint32_t idesc = instr_desc<BN>();
-  constexpr uint32_t TX = C::A_BYTES + C::B_BYTES;
+  const uint32_t tmem = ctrl->tmem;
+  auto stage = [&](int s) { return smem + s * C::STAGE; };
+  const int nk = p.nk;
+  volatile int* ab = &ctrl->abort;
 
-  auto stage_ptr = [&](int s) { return smem + s * C::STAGE; };
-  // producer prologue
-  int issued = 0;
-  if (tid == 0) {
-    for (; issued < S && issued < nkb; ++issued) {
-      const int s = issued;
-      const uint32_t a = smem_u32(stage_ptr(s));
-      mbar_expect_tx(full0 + 8 * s, TX);
-      tma_load_3d(a, &tmA, (kb0 + issued) * BK, row0, z, full0 + 8 * s);
-      tma_load_3d(a + 2 * C::A_BYTES, &tmB, (kb0 + issued) * BK, col0, zb, full0 + 8 * s);
-    }
-  }
-
-  double acc64[MODE == kGram ? BN : 1];
-#pragma unroll
-  for (int c = 0; c < (MODE == kGram ? BN : 1); ++c) acc64[c] = 0.0;
-  int flushes = 0;
-  bool chain_start = true;
-  int mma_commits = 0;
-
-  int consumed = 0;  // k-blocks whose full barrier every thread has passed
-  for (int i = 0; i < nkb; ++i) {
-    const int s = i % S;
-    const uint32_t ph = (i / S) & 1;
-    const bool ok = mbar_wait(full0 + 8 * s, ph, abort);
-    if (!ok) {
-      if (p.error) atomicExch(p.error, 1);
-      *abort = 1;
-    } else {
-      // split the tile: hi in place, lo into the sibling buffer
-      float4* a = reinterpret_cast<float4*>(stage_ptr(s));
-      float4* alo = reinterpret_cast<float4*>(stage_ptr(s) + C::A_BYTES);
-      float4* b = reinterpret_cast<float4*>(stage_ptr(s) + 2 * C::A_BYTES);
-      float4* blo = reinterpret_cast<float4*>(stage_ptr(s) + 2 * C::A_BYTES + C::B_BYTES);
-#pragma unroll 4
-      for (int k = tid; k < C::A_BYTES / 16; k += THREADS) {
-        float4 v = a[k], lo;
-        split4(v, lo);
-        a[k] = v;
-        alo[k] = lo;
-      }
-#pragma unroll 4
-      for (int k = tid; k < C::B_BYTES / 16; k += THREADS) {
-        float4 v = b[k], lo;
-        split4(v, lo);
-        b[k] = v;
-        blo[k] = lo;
-      }
-    }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    fence_before_sync();
-    __syncthreads();
-    if (*abort) break;  // uniform: read after the barrier
-    consumed = i + 1;
-    if (tid == 0) {
-      fence_after_sync();
-      const uint32_t ahi = smem_u32(stage_ptr(s)), alo = ahi + C::A_BYTES;
-      const uint32_t bhi = ahi + 2 * C::A_BYTES, blo = bhi + C::B_BYTES;
-#pragma unroll
-      for (int kk = 0; kk < BK / 8; ++kk) {
-        const uint32_t off = kk * 32;  // 8 tf32 = 32 bytes along K
-        mma_tf32(tmem, smem_desc(alo + off), smem_desc(bhi + off), idesc,
-                 (chain_start && kk == 0) ? 0u : 1u);
-        mma_tf32(tmem, smem_desc(ahi + off), smem_desc(blo + off), idesc, 1u);
-        mma_tf32(tmem, smem_desc(ahi + off), smem_desc(bhi + off), idesc, 1u);
-      }
-      mma_commit(empty0 + 8 * s);
-      ++mma_commits;
-      // refill the stage the previous k-block used
-      if (i >= 1) {
-        const int j = i - 1 + S;
-        const int sp = (i - 1) % S;
-        if (j < nkb) {
-          if (!mbar_wait(empty0 + 8 * sp, ((i - 1) / S) & 1, abort)) {
-            if (p.error) atomicExch(p.error, 2);
-            *abort = 1;
-          } else {
-            const uint32_t a = smem_u32(stage_ptr(sp));
-            mbar_expect_tx(full0 + 8 * sp, TX);
-            tma_load_3d(a, &tmA, (kb0 + j) * BK, row0, z, full0 + 8 * sp);
-            tma_load_3d(a + 2 * C::A_BYTES, &tmB, (kb0 + j) * BK, col0, zb, full0 + 8 * sp);
-            ++issued;
+  if (warp == 0) {
+    if (lane == 0) {  // producer
+      int g = 0;
+      for (int item = blockIdx.x; item < p.nitems && !aborted(ctrl); item += gridDim.x) {
+        const int z = item / p.nqt, qt = item % p.nqt, mol = z / p.nao;
+        for (int kb = 0; kb < nk; ++kb, ++g) {
+          const int s = g % S;
+          if (g >= S && !mbar_wait(empty0 + 8 * s, ((g / S) - 1) & 1, ab)) {
+            set_abort(ctrl, p.error, 11);
+            break;
           }
+          const uint32_t a = smem_u32(stage(s));
+          mbar_expect_tx(full0 + 8 * s, C::A_BYTES + 2 * C::C_BYTES);
+          tma_load_3d(a, &tmA, kb * BK, qt * BM, z, full0 + 8 * s);
+          tma_load_3d(a + 2 * C::A_BYTES, &tmCh, kb * BK, 0, mol, full0 + 8 * s);
+          tma_load_3d(a + 2 * C::A_BYTES + C::C_BYTES, &tmCl, kb * BK, 0, mol, full0 + 8 * s);
+          *reinterpret_cast<volatile int*>(&ctrl->issued) = g + 1;
         }
       }
     }
-    chain_start = false;
-    const bool last = (i == nkb - 1);
-    if (MODE == kGram && ((i + 1) % kFlush == 0 || last)) {
-      if (tid == 0) mma_commit(accb);
-      if (!mbar_wait(accb, flushes & 1, abort)) {
-        if (p.error) atomicExch(p.error, 3);
-        *abort = 1;
+  } else if (warp >= 1 && warp <= 4) {  // splitters
+    const int ts = tid - 32;
+    int g = 0;
+    for (int item = blockIdx.x; item < p.nitems; item += gridDim.x) {
+      for (int kb = 0; kb < nk; ++kb, ++g) {
+        const int s = g % S;
+        if (!mbar_wait(full0 + 8 * s, (g / S) & 1, ab)) {
+          set_abort(ctrl, p.error, 12);
+          goto split_done;
+        }
+        if (ts == 0) *reinterpret_cast<volatile int*>(&ctrl->consumed) = g + 1;
+        float4* a = reinterpret_cast<float4*>(stage(s));
+        float4* alo = reinterpret_cast<float4*>(stage(s) + C::A_BYTES);
+#pragma unroll 4
+        for (int k = ts; k < C::A_BYTES / 16; k += 128) {
+          float4 v = a[k], lo;
+          split4(v, lo);
+          a[k] = v;
+          alo[k] = lo;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(conv0 + 8 * s);
       }
-      __syncthreads();
-      if (*abort) break;  // uniform
-      ++flushes;
+    }
+  split_done:;
+  } else if (warp == 5) {
+    if (lane == 0) {  // MMA issuer
+      constexpr uint32_t idesc = instr_desc<BN>();
+      int g = 0, t = 0;
+      for (int item = blockIdx.x; item < p.nitems && !aborted(ctrl); item += gridDim.x, ++t) {
+        const int b = t & 1;
+        if (t >= 2 && !mbar_wait(ae0 + 8 * b, ((t >> 1) - 1) & 1, ab)) {
+          set_abort(ctrl, p.error, 13);
+          break;
+        }
+        fence_after_sync();
+        const uint32_t dt = tmem + b * kTmemBuf;
+        bool ok = true;
+        for (int kb = 0; kb < nk; ++kb, ++g) {
+          const int s = g % S;
+          if (!mbar_wait(conv0 + 8 * s, (g / S) & 1, ab)) {
+            set_abort(ctrl, p.error, 14);
+            ok = false;
+            break;
+          }
+          fence_after_sync();
+          const uint32_t ahi = smem_u32(stage(s)), alo = ahi + C::A_BYTES;
+          const uint32_t chi = ahi + 2 * C::A_BYTES, clo = chi + C::C_BYTES;
+#pragma unroll
+          for (int kk = 0; kk < BK / 8; ++kk) {
+            const uint32_t off = kk * 32;
+            mma_tf32(dt, smem_desc(alo + off), smem_desc(chi + off), idesc,
+                     (kb == 0 && kk == 0) ? 0u : 1u);
+            mma_tf32(dt, smem_desc(ahi + off), smem_desc(clo + off), idesc, 1u);
+            mma_tf32(dt, smem_desc(ahi + off), smem_desc(chi + off), idesc, 1u);
+          }
+          mma_commit(empty0 + 8 * s);
+          *reinterpret_cast<volatile int*>(&ctrl->commits) = g + 1;
+        }
+        if (!ok) break;
+        mma_commit(af0 + 8 * b);
+      }
+    }
+  } else {  // epilogue warps 6..9
+    const int q = warp & 3;  // TMEM lane quarter this warp may access
+    int t = 0;
+    for (int item = blockIdx.x; item < p.nitems; item += gridDim.x, ++t) {
+      const int b = t & 1;
+      if (!mbar_wait(af0 + 8 * b, (t >> 1) & 1, ab)) {
+        set_abort(ctrl, p.error, 15);
+        break;
+      }
       fence_after_sync();
+      const int z = item / p.nqt, qt = item % p.nqt;
+      const int row = qt * BM + q * 32 + lane;
+      const bool valid = row < p.naux;
+      double rho_part = 0.0;
+      float* uh = p.u_hi + ((size_t)z * p.naux + (valid ? row : 0)) * p.ldu;
+      float* ul = p.u_lo + ((size_t)z * p.naux + (valid ? row : 0)) * p.ldu;
+      const double* cv = p.cvec + (size_t)z * p.nocc;
 #pragma unroll
       for (int c = 0; c < BN; c += 16) {
         float v[16];
-        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + c, v);
+        tmem_ld16(tmem + b * kTmemBuf + ((uint32_t)(q * 32) << 16) + c, v);
+        if (valid) {
 #pragma unroll
-        for (int q = 0; q < 16; ++q) acc64[c + q] += (double)v[q];
+          for (int k = 0; k < 16; ++k) {
+            const int col = c + k;
+            if (col < p.ldu) {
+              const float h = rn_tf32(v[k]);
+              uh[col] = h;
+              ul[col] = rn_tf32(v[k] - h);
+            }
+            if (col < p.nocc) rho_part += (double)v[k] * cv[col];
+          }
+        }
       }
       fence_before_sync();
-      __syncthreads();
-      chain_start = true;
-    }
-  }
-  // the barrier-read flag is uniform from here on
-  __syncthreads();
-
-  if (!*abort && MODE == kHalf) {
-    if (tid == 0) mma_commit(accb);
-    if (!mbar_wait(accb, 0, abort)) {
-      if (p.error) atomicExch(p.error, 4);
-      *abort = 1;
-    }
-    __syncthreads();
-    if (!*abort) {
-      fence_after_sync();
-      const int row = row0 + tid;
-      double rho_part = 0.0;
-#pragma unroll
-      for (int c = 0; c < BN; c += 16) {
-        float v[16];
-        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + c, v);
-        if (row < p.m) {
-          float* dst = p.u + ((size_t)z * p.m + row) * p.ldu;
-#pragma unroll
-          for (int q = 0; q < 16; ++q) {
-            const int col = col0 + c + q;
-            if (col < p.ldu) dst[col] = v[q];
-            if (col < p.ncvec) rho_part += (double)v[q] * p.cvec[(size_t)z * p.cld + col];
-          }
-        }
-      }
-      if (row < p.m && p.rho) atomicAdd(p.rho + (size_t)(z / p.rho_div) * p.m + row, 2.0 * rho_part);
-    }
-  }
-  if (!*abort && MODE == kGram) {
-    const int row = row0 + tid;
-    if (row < p.m) {
-      double* dst = p.kout + ((size_t)z * p.m + row) * p.n;
-#pragma unroll
-      for (int c = 0; c < BN; ++c) {
-        const int col = col0 + c;
-        if (col < p.n) atomicAdd(dst + col, acc64[c]);
-      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(ae0 + 8 * b);
+      if (valid && p.rho) atomicAdd(p.rho + (size_t)(z / p.nao) * p.naux + row, 2.0 * rho_part);
     }
   }
 
-  if (*abort && tid == 0) {
-    // drain: copies still in flight land in this CTA's shared memory and the
-    // last committed MMAs still read it and write TMEM; wait for both (bounded)
-    volatile int never = 0;
-    for (int i2 = consumed; i2 < issued; ++i2)
-      mbar_wait(full0 + 8 * (i2 % S), (i2 / S) & 1, &never);
-    if (mma_commits > 0) {
-      const int lastc = mma_commits - 1;
-      mbar_wait(empty0 + 8 * (lastc % S), (lastc / S) & 1, &never);
-    }
-  }
   fence_before_sync();
+  __syncthreads();
+  if (aborted(ctrl) && tid == 0) {
+    // bounded drain of copies and MMAs still in flight
+    int never = 0;
+    const int issued = ctrl->issued, consumed = ctrl->consumed;
+    for (int g = consumed; g < issued; ++g)
+      mbar_wait(full0 + 8 * (g % S), (g / S) & 1, &never);
+    if (ctrl->commits > 0) {
+      const int lc = ctrl->commits - 1;
+      mbar_wait(empty0 + 8 * (lc % S), (lc / S) & 1, &never);
+    }
+  }
   __syncthreads();
   if (warp == 0) {
     fence_after_sync();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                 "r"(C::TMEM_COLS)
+                 "r"(2 * kTmemBuf)
                  : "memory");
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Gram product: K[z] += U U^T over kdim with pre-split U (hi, lo) in HBM;
+// upper-triangle 128x128 tiles, split K range; warp roles:
+//   w0 TMA producer, w1 MMA issuer, w2-w9 epilogue (two column halves per
+//   TMEM lane quarter; FP64 accumulators drained every kGramFlush K-blocks)
+// ---------------------------------------------------------------------------
+
+constexpr int kGramFlush = 2;
+
+struct GramCfg {
+  static constexpr int TILE = BM * BK * 4;  // 16 KB
+  static constexpr int STAGE = 4 * TILE;    // A hi, A lo, B hi, B lo
+  static constexpr int S = 3;
+  static constexpr int SMEM = S * STAGE + 1024 + (int)sizeof(Ctrl) + 64;
+};
+
+struct GramParams {
+  int nao, kdim, ntiles_ut, nt, kblocks_per_split, ksplit;
+  double* kout;
+  int* error;
+};
+
+__global__ void __launch_bounds__(kGramThreads, 1)
+    gram_ws_kernel(const __grid_constant__ CUtensorMap tmH, const __grid_constant__ CUtensorMap tmL,
+                   GramParams p) {
+  using C = GramCfg;
+  constexpr int S = C::S;
+  constexpr int BN = 128;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  Ctrl* ctrl = reinterpret_cast<Ctrl*>(smem + S * C::STAGE);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  // decode (upper-triangle tile, molecule, split)
+  const int tile = blockIdx.x;
+  int mt = 0, rem = tile;
+  while (rem >= p.nt - mt) {
+    rem -= p.nt - mt;
+    ++mt;
+  }
+  const int nt = mt + rem;
+  const int z = blockIdx.y / p.ksplit, split = blockIdx.y % p.ksplit;
+  const int kb_total = (p.kdim + BK - 1) / BK;
+  const int kb0 = split * p.kblocks_per_split;
+  const int kb1 = min(kb_total, kb0 + p.kblocks_per_split);
+  const int nkb = kb1 - kb0;
+  if (nkb <= 0 || mt >= p.nt) return;
+  const int nchains = (nkb + kGramFlush - 1) / kGramFlush;
+
+  const uint32_t full0 = smem_u32(ctrl->full), empty0 = smem_u32(ctrl->empty);
+  const uint32_t af0 = smem_u32(ctrl->acc_full), ae0 = smem_u32(ctrl->acc_empty);
+  if (tid == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(full0 + 8 * s, 1);
+      mbar_init(empty0 + 8 * s, 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(af0 + 8 * b, 1);
+      mbar_init(ae0 + 8 * b, 8);
+    }
+    ctrl->abort = 0;
+    ctrl->issued = ctrl->consumed = ctrl->commits = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&ctrl->tmem)),
+                 "r"(2 * kTmemBuf)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  const uint32_t tmem = ctrl->tmem;
+  auto stage = [&](int s) { return smem + s * C::STAGE; };
+  volatile int* ab = &ctrl->abort;
+  double acc[64];
+#pragma unroll
+  for (int c = 0; c < 64; ++c) acc[c] = 0.0;
+
+  if (warp == 0) {
+    if (lane == 0) {  // producer
+      for (int i = 0; i < nkb; ++i) {
+        const int s = i % S;
+        if (i >= S && !mbar_wait(empty0 + 8 * s, ((i / S) - 1) & 1, ab)) {
+          set_abort(ctrl, p.error, 21);
+          break;
+        }
+        const uint32_t a = smem_u32(stage(s));
+        const int k = (kb0 + i) * BK;
+        mbar_expect_tx(full0 + 8 * s, C::STAGE);
+        tma_load_3d(a, &tmH, k, mt * BM, z, full0 + 8 * s);
+        tma_load_3d(a + C::TILE, &tmL, k, mt * BM, z, full0 + 8 * s);
+        tma_load_3d(a + 2 * C::TILE, &tmH, k, nt * BN, z, full0 + 8 * s);
+        tma_load_3d(a + 3 * C::TILE, &tmL, k, nt * BN, z, full0 + 8 * s);
+        *reinterpret_cast<volatile int*>(&ctrl->issued) = i + 1;
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {  // MMA issuer
+      constexpr uint32_t idesc = instr_desc<BN>();
+      int i = 0;
+      for (int ch = 0; ch < nchains && !aborted(ctrl); ++ch) {
+        const int b = ch & 1;
+        if (ch >= 2 && !mbar_wait(ae0 + 8 * b, ((ch >> 1) - 1) & 1, ab)) {
+          set_abort(ctrl, p.error, 22);
+          break;
+        }
+        fence_after_sync();
+        const uint32_t dt = tmem + b * kTmemBuf;
+        const int iend = min(nkb, i + kGramFlush);
+        bool ok = true;
+        for (int first = i; i < iend; ++i) {
+          const int s = i % S;
+          if (!mbar_wait(full0 + 8 * s, (i / S) & 1, ab)) {
+            set_abort(ctrl, p.error, 23);
+            ok = false;
+            break;
+          }
+          *reinterpret_cast<volatile int*>(&ctrl->consumed) = i + 1;
+          fence_after_sync();
+          const uint32_t ahi = smem_u32(stage(s)), alo = ahi + C::TILE;
+          const uint32_t bhi = ahi + 2 * C::TILE, blo = ahi + 3 * C::TILE;
+#pragma unroll
+          for (int kk = 0; kk < BK / 8; ++kk) {
+            const uint32_t off = kk * 32;
+            mma_tf32(dt, smem_desc(alo + off), smem_desc(bhi + off), idesc,
+                     (i == first && kk == 0) ? 0u : 1u);
+            mma_tf32(dt, smem_desc(ahi + off), smem_desc(blo + off), idesc, 1u);
+            mma_tf32(dt, smem_desc(ahi + off), smem_desc(bhi + off), idesc, 1u);
+          }
+          mma_commit(empty0 + 8 * s);
+          *reinterpret_cast<volatile int*>(&ctrl->commits) = i + 1;
+        }
+        if (!ok) break;
+        mma_commit(af0 + 8 * b);
+      }
+    }
+  } else {  // epilogue warps 2..9
+    const int q = warp & 3, half = (warp - 2) >> 2;
+    for (int ch = 0; ch < nchains; ++ch) {
+      const int b = ch & 1;
+      if (!mbar_wait(af0 + 8 * b, (ch >> 1) & 1, ab)) {
+        set_abort(ctrl, p.error, 24);
+        break;
+      }
+      fence_after_sync();
+#pragma unroll
+      for (int c = 0; c < 64; c += 16) {
+        float v[16];
+        tmem_ld16(tmem + b * kTmemBuf + half * 64 + c + ((uint32_t)(q * 32) << 16), v);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) acc[c + k] += (double)v[k];
+      }
+      fence_before_sync();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(ae0 + 8 * b);
+    }
+    if (!aborted(ctrl)) {
+      const int row = mt * BM + q * 32 + lane;
+      if (row < p.nao) {
+        double* base = p.kout + (size_t)z * p.nao * p.nao;
+#pragma unroll
+        for (int c = 0; c < 64; ++c) {
+          const int col = nt * BN + half * 64 + c;
+          if (col < p.nao) {
+            atomicAdd(base + (size_t)row * p.nao + col, acc[c]);
+            if (mt != nt) atomicAdd(base + (size_t)col * p.nao + row, acc[c]);
+          }
+        }
+      }
+    }
+  }
+
+  fence_before_sync();
+  __syncthreads();
+  if (aborted(ctrl) && tid == 0) {
+    int never = 0;
+    const int issued = ctrl->issued, consumed = ctrl->consumed;
+    for (int g = consumed; g < issued; ++g)
+      mbar_wait(full0 + 8 * (g % S), (g / S) & 1, &never);
+    if (ctrl->commits > 0) {
+      const int lc = ctrl->commits - 1;
+      mbar_wait(empty0 + 8 * (lc % S), (lc / S) & 1, &never);
+    }
+  }
+  __syncthreads();
+  if (warp == 0) {
+    fence_after_sync();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(2 * kTmemBuf)
+                 : "memory");
+  }
+}
+
+__global__ void split_tf32_kernel(const float* __restrict__ x, float* __restrict__ hi,
+                                  float* __restrict__ lo, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const float h = rn_tf32(x[i]);
+    hi[i] = h;
+    lo[i] = rn_tf32(x[i] - h);
   }
 }
 
@@ -432,20 +637,27 @@ static int make_map(CUtensorMap* tm, const float* base, int kext, int ld, int ro
   return VQC_STATUS_SUCCESS;
 }
 
-template <int BN, int MODE>
-static int launch(const CUtensorMap& ta, const CUtensorMap& tb, const Params& p, dim3 grid,
-                  cudaStream_t st) {
-  using C = Cfg<BN>;
-  auto k = tf32x3_gemm_kernel<BN, MODE>;
+static int sm_count() {
+  int sms = 148, dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms;
+}
+
+template <int BN>
+static int launch_half(const CUtensorMap& ta, const CUtensorMap& th, const CUtensorMap& tl,
+                       const HalfParams& p, cudaStream_t st) {
+  using C = HalfCfg<BN>;
   static bool attr = false;
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
-    if (e != cudaSuccess) return cuda_status(e, "tf32x3 smem attribute");
+    cudaError_t e = cudaFuncSetAttribute(half_ws_kernel<BN>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
+    if (e != cudaSuccess) return cuda_status(e, "half smem attribute");
     attr = true;
   }
-  k<<<grid, THREADS, C::SMEM, st>>>(ta, tb, p);
+  const int grid = p.nitems < sm_count() ? p.nitems : sm_count();
+  half_ws_kernel<BN><<<grid, kHalfThreads, C::SMEM, st>>>(ta, th, tl, p);
   count_launch();
-  return cuda_status(cudaGetLastError(), "tf32x3 launch");
+  return cuda_status(cudaGetLastError(), "half launch");
 }
 
 }  // namespace tc
@@ -454,80 +666,96 @@ static int launch(const CUtensorMap& ta, const CUtensorMap& tb, const Params& p,
 using namespace vqc;
 using namespace vqc::tc;
 
+extern "C" int vqc_split_tf32(const float* x, float* hi, float* lo, int64_t n, void* stream) {
+  if (!x || !hi || !lo || n < 0) return fail(VQC_STATUS_INVALID_ARGUMENT, "split_tf32: bad argument");
+  if (n == 0) return VQC_STATUS_SUCCESS;
+  long long blocks = (n + 255) / 256;
+  blocks = blocks > 4096 ? 4096 : blocks;
+  split_tf32_kernel<<<(int)blocks, 256, 0, (cudaStream_t)stream>>>(x, hi, lo, (size_t)n);
+  count_launch();
+  return cuda_status(cudaGetLastError(), "split_tf32");
+}
+
 extern "C" int vqc_tc_half_transform(const float* b_aux_major, int32_t nmol, int32_t nao,
-                                     int32_t ld_ao, int32_t naux, const float* ct,
-                                     const double* c_occ, int32_t nocc, int32_t o_pad, float* u,
-                                     double* rho, int32_t* error, void* stream) {
-  if (!b_aux_major || !ct || !c_occ || !u || nmol <= 0 || nao <= 0 || naux <= 0 || nocc <= 0 ||
-      o_pad < nocc || o_pad % 16 || o_pad > 128 || ld_ao < nao)
+                                     int32_t ld_ao, int32_t naux, const float* ct_hi,
+                                     const float* ct_lo, const double* c_occ, int32_t nocc,
+                                     int32_t o_pad, float* u_hi, float* u_lo, double* rho,
+                                     int32_t* error, void* stream) {
+  if (!b_aux_major || !ct_hi || !ct_lo || !c_occ || !u_hi || !u_lo || nmol <= 0 || nao <= 0 ||
+      naux <= 0 || nocc <= 0 || o_pad < nocc || o_pad % 16 || o_pad > 128 || ld_ao < nao)
     return fail(VQC_STATUS_INVALID_ARGUMENT, "half_transform: bad argument");
-  CUtensorMap ta, tb;
+  CUtensorMap ta, th, tl;
   int st = make_map(&ta, b_aux_major, nao, ld_ao, naux, nmol * nao, BM);
-  if (!st) st = make_map(&tb, ct, nao, ld_ao, nocc, nmol, o_pad);
+  if (!st) st = make_map(&th, ct_hi, nao, ld_ao, nocc, nmol, o_pad);
+  if (!st) st = make_map(&tl, ct_lo, nao, ld_ao, nocc, nmol, o_pad);
   if (st) return st;
-  Params p{};
-  p.m = naux;
-  p.n = o_pad;
-  p.kdim = nao;
-  p.kblocks_per_split = (nao + BK - 1) / BK;
-  p.ksplit = 1;
-  p.b_batch_div = nao;
-  p.u = u;
+  HalfParams p{};
+  p.nao = nao;
+  p.naux = naux;
+  p.nocc = nocc;
   p.ldu = o_pad;
+  p.nqt = (naux + BM - 1) / BM;
+  const long long items = (long long)nmol * nao * p.nqt;
+  if (items > 0x7fffffffLL) return fail(VQC_STATUS_INVALID_ARGUMENT, "half_transform: too many tiles");
+  p.nitems = (int)items;
+  p.nk = (nao + BK - 1) / BK;
+  p.u_hi = u_hi;
+  p.u_lo = u_lo;
   p.rho = rho;
   p.cvec = c_occ;
-  p.cld = nocc;
-  p.ncvec = nocc;
-  p.rho_div = nao;
   p.error = error;
-  if ((long long)nmol * nao > 65535) return fail(VQC_STATUS_INVALID_ARGUMENT, "half_transform: grid too large");
-  dim3 grid((naux + BM - 1) / BM, 1, nmol * nao);
   cudaStream_t s = (cudaStream_t)stream;
   switch (o_pad) {
-    case 16: return launch<16, kHalf>(ta, tb, p, grid, s);
-    case 32: return launch<32, kHalf>(ta, tb, p, grid, s);
-    case 48: return launch<48, kHalf>(ta, tb, p, grid, s);
-    case 64: return launch<64, kHalf>(ta, tb, p, grid, s);
-    case 80: return launch<80, kHalf>(ta, tb, p, grid, s);
-    case 96: return launch<96, kHalf>(ta, tb, p, grid, s);
-    case 112: return launch<112, kHalf>(ta, tb, p, grid, s);
-    case 128: return launch<128, kHalf>(ta, tb, p, grid, s);
+    case 16: return launch_half<16>(ta, th, tl, p, s);
+    case 32: return launch_half<32>(ta, th, tl, p, s);
+    case 48: return launch_half<48>(ta, th, tl, p, s);
+    case 64: return launch_half<64>(ta, th, tl, p, s);
+    case 80: return launch_half<80>(ta, th, tl, p, s);
+    case 96: return launch_half<96>(ta, th, tl, p, s);
+    case 112: return launch_half<112>(ta, th, tl, p, s);
+    case 128: return launch_half<128>(ta, th, tl, p, s);
   }
   return fail(VQC_STATUS_INVALID_ARGUMENT, "half_transform: o_pad");
 }
 
-extern "C" int vqc_tc_gram(const float* u, int32_t nmol, int32_t nao, int32_t kdim, double* kout,
-                           int32_t* error, void* stream) {
-  if (!u || !kout || nmol <= 0 || nao <= 0 || kdim <= 0 || kdim % 4)
+extern "C" int vqc_tc_gram(const float* u_hi, const float* u_lo, int32_t nmol, int32_t nao,
+                           int32_t kdim, double* kout, int32_t* error, void* stream) {
+  if (!u_hi || !u_lo || !kout || nmol <= 0 || nao <= 0 || kdim <= 0 || kdim % 4)
     return fail(VQC_STATUS_INVALID_ARGUMENT, "gram: bad argument");
-  constexpr int BN = 64;
-  CUtensorMap ta, tb;
-  int st = make_map(&ta, u, kdim, kdim, nao, nmol, BM);
-  if (!st) st = make_map(&tb, u, kdim, kdim, nao, nmol, BN);
+  CUtensorMap th, tl;
+  int st = make_map(&th, u_hi, kdim, kdim, nao, nmol, BM);
+  if (!st) st = make_map(&tl, u_lo, kdim, kdim, nao, nmol, BM);
   if (st) return st;
-  const int mt = (nao + BM - 1) / BM, nt = (nao + BN - 1) / BN;
+  const int nt = (nao + BM - 1) / BM;
+  const int tiles = nt * (nt + 1) / 2;
   const int kb_total = (kdim + BK - 1) / BK;
-  int sms = 148;
-  int dev = 0;
-  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const long long tiles = (long long)mt * nt * nmol;
-  int ksplit = (int)((2LL * sms + tiles - 1) / tiles);
-  ksplit = ksplit < 1 ? 1 : ksplit;
-  const int max_split = (kb_total + kFlush - 1) / kFlush;
-  ksplit = ksplit > max_split ? max_split : ksplit;
+  const int sms = sm_count();
+  long long base = (long long)tiles * nmol;
+  int ksplit = (int)((2LL * sms + base - 1) / base);
+  const int max_split = (kb_total + kGramFlush - 1) / kGramFlush;
+  ksplit = ksplit < 1 ? 1 : (ksplit > max_split ? max_split : ksplit);
   int per = (kb_total + ksplit - 1) / ksplit;
-  per = (per + kFlush - 1) / kFlush * kFlush;
+  per = (per + kGramFlush - 1) / kGramFlush * kGramFlush;
   ksplit = (kb_total + per - 1) / per;
-  Params p{};
-  p.m = nao;
-  p.n = nao;
+  if ((long long)nmol * ksplit > 65535) return fail(VQC_STATUS_INVALID_ARGUMENT, "gram: grid too large");
+  GramParams p{};
+  p.nao = nao;
   p.kdim = kdim;
+  p.nt = nt;
+  p.ntiles_ut = tiles;
   p.kblocks_per_split = per;
   p.ksplit = ksplit;
-  p.b_batch_div = 1;
   p.kout = kout;
   p.error = error;
-  if ((long long)nmol * ksplit > 65535) return fail(VQC_STATUS_INVALID_ARGUMENT, "gram: grid too large");
-  dim3 grid(mt, nt, nmol * ksplit);
-  return launch<BN, kGram>(ta, tb, p, grid, (cudaStream_t)stream);
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(gram_ws_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         GramCfg::SMEM);
+    if (e != cudaSuccess) return cuda_status(e, "gram smem attribute");
+    attr = true;
+  }
+  dim3 grid(tiles, nmol * ksplit);
+  gram_ws_kernel<<<grid, kGramThreads, GramCfg::SMEM, (cudaStream_t)stream>>>(th, tl, p);
+  count_launch();
+  return cuda_status(cudaGetLastError(), "gram launch");
 }

@@ -92,7 +92,8 @@ class MixedBuilder:
         self.st = torch.cuda.current_stream().cuda_stream
         _lib.call("vqc_unpack_aux_major", b_packed.contiguous().data_ptr(), nb, n, x, self.ld,
                   self.b.data_ptr(), self.st)
-        self.u = torch.empty(nb, n, x, self.o_pad, dtype=torch.float32, device=dev)
+        self.u_hi = torch.empty(nb, n, x, self.o_pad, dtype=torch.float32, device=dev)
+        self.u_lo = torch.empty_like(self.u_hi)
         self.rho = torch.empty(nb, x, dtype=torch.float64, device=dev)
         # the FP64 whitened rows stay resident for the refinement iterations,
         # the final energy and the gradient
@@ -109,12 +110,17 @@ class MixedBuilder:
         nb, n, o = self.nb, self.n, self.nocc
         ct = torch.zeros(nb, o, self.ld, dtype=torch.float32, device=c_occ.device)
         ct[:, :, :n] = c_occ.transpose(1, 2)
+        ct_hi = torch.empty_like(ct)
+        ct_lo = torch.empty_like(ct)
+        self._lib.call("vqc_split_tf32", ct.data_ptr(), ct_hi.data_ptr(), ct_lo.data_ptr(),
+                       ct.numel(), self.st)
         c64 = c_occ.contiguous()
         self.rho.zero_()
         with TIMER.stage("K_half_tc"):
             self._lib.call("vqc_tc_half_transform", self.b.data_ptr(), nb, n, self.ld, self.x,
-                           ct.data_ptr(), c64.data_ptr(), o, self.o_pad, self.u.data_ptr(),
-                           self.rho.data_ptr(), self.err.data_ptr(), self.st)
+                           ct_hi.data_ptr(), ct_lo.data_ptr(), c64.data_ptr(), o, self.o_pad,
+                           self.u_hi.data_ptr(), self.u_lo.data_ptr(), self.rho.data_ptr(),
+                           self.err.data_ptr(), self.st)
 
     def build(self, d: torch.Tensor, c_occ: torch.Tensor):
         nb, n = self.nb, self.n
@@ -125,8 +131,8 @@ class MixedBuilder:
                            self.ld, self.x, j.data_ptr(), self.st)
         k = torch.zeros(nb, n, n, dtype=torch.float64, device=d.device)
         with TIMER.stage("K_gram_tc"):
-            self._lib.call("vqc_tc_gram", self.u.data_ptr(), nb, n, self.x * self.o_pad,
-                           k.data_ptr(), self.err.data_ptr(), self.st)
+            self._lib.call("vqc_tc_gram", self.u_hi.data_ptr(), self.u_lo.data_ptr(), nb, n,
+                           self.x * self.o_pad, k.data_ptr(), self.err.data_ptr(), self.st)
         self.nbuild += 1
         self._check()
         return j, 2.0 * k

@@ -324,17 +324,28 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
     f_final = torch.zeros_like(d)
     errs, focks = [], []
     comm_tol = 10.0 * min(1e-8, density_tolerance)
-    # mixed precision: tensor-core iterations until the loose criteria below
-    # hold for every active molecule, then FP64-arithmetic refinement
-    # iterations (same FP32 B) under the standard criteria
-    exact = jk.precision != "mixed"
+    # mixed precision runs three phases per chunk:
+    #   "tc":        tensor-core J/K until |dE| < 1e-6 and max|FDS-SDF| <= 1e-4
+    #                for every active molecule (or MIXED_ITERATION_CAP);
+    #   "corrected": tensor-core J/K plus the defect dJ, dK = (FP64 - tensor core)
+    #                measured once at the switch density, until |dE| < 1e-9 and
+    #                max|FDS-SDF| <= 1e-6 (or the same cap);
+    #   "exact":     FP64 J/K from the FP64 whitened rows under the standard
+    #                criteria (usually one or two iterations).
+    phase = "tc" if jk.precision == "mixed" else "exact"
     mixed_iterations = 0
+    phase_iterations = 0
+    dj = dk = None
     for it in range(1, max_iterations + 1):
-        if exact:
+        if phase == "exact":
             j, k = jk.build_exact(d, c)
         else:
             j, k = jk.build(d, c)
             mixed_iterations += 1
+            if phase == "corrected":
+                j = j + dj
+                k = k + dk
+        phase_iterations += 1
         TIMER_ctx = TIMER.stage("scf_other")
         TIMER_ctx.__enter__()
         f = h + j - 0.5 * k
@@ -356,11 +367,19 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
         drms = ((d_new - d) ** 2).mean(dim=(1, 2)).sqrt()
         cmax = comm.abs().amax(dim=(1, 2))
         done = (de < energy_tolerance) & (drms < density_tolerance) & (cmax <= comm_tol)
-        if not exact:
+        if phase == "tc":
             loose = (de < 1e-6) & (cmax <= 1e-4)
-            if bool((loose | ~active).all()) or mixed_iterations >= MIXED_ITERATION_CAP:
-                exact = True
-                errs, focks = [], []  # restart DIIS on the refined operators
+            if bool((loose | ~active).all()) or phase_iterations >= MIXED_ITERATION_CAP:
+                je, ke = jk.build_exact(d, c)
+                dj, dk = je - j, ke - k
+                del je, ke
+                phase, phase_iterations = "corrected", 0
+                errs, focks = [], []  # restart DIIS on the corrected operators
+            done = torch.zeros_like(done)
+        elif phase == "corrected":
+            tight = (de < 1e-9) & (cmax <= 1e-6)
+            if bool((tight | ~active).all()) or phase_iterations >= MIXED_ITERATION_CAP:
+                phase, phase_iterations = "exact", 0
             done = torch.zeros_like(done)
         newly = done & active
         # record the state of molecules that are still active
