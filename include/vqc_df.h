@@ -142,13 +142,14 @@ int vqc_sp2_update(const double* x, const double* x2, double* xout, int32_t nmol
  * plan (src/scf/cuda/df_plan_setup.cpp:70,224).
  *   vqc_unpack_aux_major: packed whitened FP64 rows -> b_aux_major (FP32).
  *   vqc_split_tf32: hi = rn_tf32(x), lo = rn_tf32(x - hi) (n FP32 values).
- *   vqc_tc_half_transform: U[mol][mu][Q][i] = sum_nu B[mu][Q][nu] C[nu][i]
- *     (3xTF32 tcgen05, i < o_pad, o_pad % 16 == 0, <= 128), written split as
- *     u_hi/u_lo (FP32, TF32-representable), and rho[mol][Q] += 2 sum_{mu,i}
- *     U C[mu][i]; ct_hi/ct_lo = split C^T [mol][nocc][ld_ao] FP32, c_occ = C
- *     [mol][nao][nocc] FP64.  Reference
- *     src/scf/cuda/df_occupied_exchange.cpp:251-257 (U = B C).
- *   vqc_tc_gram: kout[mol] += U U^T over kdim = naux * o_pad from the split
+ *   vqc_tc_half_transform: U[mol][mu][i][Q] = sum_nu B[mu][Q][nu] C[nu][i]
+ *     (3xTF32 tcgen05; i < nocc, Q rows of length ld_aux >= naux, ld_aux % 4
+ *     == 0, padding left untouched), written split as u_hi/u_lo (FP32,
+ *     TF32-representable), and rho[mol][Q] += 2 sum_{mu,i} U C[mu][i];
+ *     ct_hi/ct_lo = split C^T [mol][nocc][ld_ao] FP32, c_occ = C
+ *     [mol][nao][nocc] FP64; o_pad = MMA N (round_up(nocc,16) <= 128).
+ *     Reference src/scf/cuda/df_occupied_exchange.cpp:251-257 (U = B C).
+ *   vqc_tc_gram: kout[mol] += U U^T over kdim = nocc * ld_aux from the split
  *     U (3xTF32, FP64 output); reference df_occupied_exchange.cpp:262-279.
  *   vqc_coulomb_fp32: J[mol][mu][nu] = sum_Q B[mu][Q][nu] rho[mol][Q] (FP64
  *     accumulate); reference src/scf/cuda/df_coulomb.cpp:24.
@@ -161,8 +162,8 @@ int vqc_unpack_aux_major(const double* b_packed, int32_t nmol, int32_t nao, int3
 int vqc_split_tf32(const float* x, float* hi, float* lo, int64_t n, void* stream);
 int vqc_tc_half_transform(const float* b_aux_major, int32_t nmol, int32_t nao, int32_t ld_ao,
                           int32_t naux, const float* ct_hi, const float* ct_lo,
-                          const double* c_occ, int32_t nocc, int32_t o_pad, float* u_hi,
-                          float* u_lo, double* rho, int32_t* error, void* stream);
+                          const double* c_occ, int32_t nocc, int32_t o_pad, int32_t ld_aux,
+                          float* u_hi, float* u_lo, double* rho, int32_t* error, void* stream);
 int vqc_tc_gram(const float* u_hi, const float* u_lo, int32_t nmol, int32_t nao, int32_t kdim,
                 double* kout, int32_t* error, void* stream);
 int vqc_coulomb_fp32(const float* b_aux_major, const double* rho, int32_t nmol, int32_t nao,

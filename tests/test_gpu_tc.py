@@ -31,12 +31,13 @@ def test_half_transform_and_gram(nb, n, x, o):
     st = torch.cuda.current_stream().cuda_stream
     ct_hi, ct_lo = torch.empty_like(ct), torch.empty_like(ct)
     _lib.call("vqc_split_tf32", ct.data_ptr(), ct_hi.data_ptr(), ct_lo.data_ptr(), ct.numel(), st)
-    u_hi = torch.full((nb, n, x, o_pad), float("nan"), dtype=torch.float32, device="cuda")
-    u_lo = torch.full_like(u_hi, float("nan"))
+    ldq = (x + 3) // 4 * 4
+    u_hi = torch.zeros((nb, n, o, ldq), dtype=torch.float32, device="cuda")
+    u_lo = torch.zeros_like(u_hi)
     rho = torch.zeros(nb, x, dtype=torch.float64, device="cuda")
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
     _lib.call("vqc_tc_half_transform", b.data_ptr(), nb, n, ld, x, ct_hi.data_ptr(),
-              ct_lo.data_ptr(), c.contiguous().data_ptr(), o, o_pad, u_hi.data_ptr(),
+              ct_lo.data_ptr(), c.contiguous().data_ptr(), o, o_pad, ldq, u_hi.data_ptr(),
               u_lo.data_ptr(), rho.data_ptr(), err.data_ptr(), st)
     torch.cuda.synchronize()
     assert int(err.item()) == 0
@@ -47,15 +48,15 @@ def test_half_transform_and_gram(nb, n, x, o):
     b64 = b[..., :n].double()
     c_used = (ct_hi + ct_lo)[:, :, :n].transpose(1, 2).double()  # the C the kernel multiplied
     ref = torch.einsum("bmqn,bni->bmqi", b64, c_used)
-    u = u_hi.double() + u_lo.double()
-    got = u[..., :o]
+    u = u_hi.double() + u_lo.double()  # (nb, mu, i, Q)
+    got = u[..., :x].transpose(2, 3)
     scale = ref.abs().max().item()
     assert (got - ref).abs().max().item() <= 5e-6 * scale
-    assert (u[..., o:] == 0).all()
+    assert (u[..., x:] == 0).all()
     ref_rho = 2.0 * torch.einsum("bmi,bmqi->bq", c, ref)
     assert (rho - ref_rho).abs().max().item() <= 5e-6 * ref_rho.abs().max().item()
 
-    kdim = x * o_pad
+    kdim = o * ldq
     k = torch.zeros(nb, n, n, dtype=torch.float64, device="cuda")
     _lib.call("vqc_tc_gram", u_hi.data_ptr(), u_lo.data_ptr(), nb, n, kdim, k.data_ptr(),
               err.data_ptr(), st)
@@ -117,8 +118,8 @@ def test_unpack_aux_major_roundtrip():
 def test_bad_arguments_rejected():
     st = torch.cuda.current_stream().cuda_stream
     with pytest.raises(_lib.VqcError):
-        _lib.call("vqc_tc_half_transform", 0, 1, 8, 8, 8, 0, 0, 0, 4, 16, 0, 0, 0, 0, st)
+        _lib.call("vqc_tc_half_transform", 0, 1, 8, 8, 8, 0, 0, 0, 4, 16, 8, 0, 0, 0, 0, st)
     x = torch.zeros(64, dtype=torch.float32, device="cuda")
     with pytest.raises(_lib.VqcError):  # o_pad above the supported tile
         _lib.call("vqc_tc_half_transform", x.data_ptr(), 1, 8, 8, 8, x.data_ptr(), x.data_ptr(),
-                  x.data_ptr(), 140, 144, x.data_ptr(), x.data_ptr(), x.data_ptr(), x.data_ptr(), st)
+                  x.data_ptr(), 140, 144, 8, x.data_ptr(), x.data_ptr(), x.data_ptr(), x.data_ptr(), st)

@@ -92,8 +92,8 @@ _SIGNATURES = {
                               ctypes.c_int32, _P, _P], ctypes.c_int),
     "vqc_split_tf32": ([_P, _P, _P, ctypes.c_int64, _P], ctypes.c_int),
     "vqc_tc_half_transform": ([_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
-                               ctypes.c_int32, _P, _P, _P, ctypes.c_int32, ctypes.c_int32, _P,
-                               _P, _P, _P, _P], ctypes.c_int),
+                               ctypes.c_int32, _P, _P, _P, ctypes.c_int32, ctypes.c_int32,
+                               ctypes.c_int32, _P, _P, _P, _P, _P], ctypes.c_int),
     "vqc_tc_gram": ([_P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _P, _P, _P],
                     ctypes.c_int),
     "vqc_coulomb_fp32": ([_P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,

@@ -9,7 +9,9 @@
 //
 //   half_ws_kernel -- U[mol][mu][Q][i] = sum_nu B[mol][mu][Q][nu] C[nu][i]
 //     (reference src/scf/cuda/df_occupied_exchange.cpp:251-257).  Persistent
-//     over (mu, 128-row Q tile) items.  Warp roles: one TMA producer, four
+//     over (mu, 128-row Q tile) items; each CTA takes a contiguous item range
+//     with mu fastest, so rho rows accumulate in registers across items.  U is
+//     written as [mol][mu][i][Q] (Q contiguous: coalesced epilogue stores).  Warp roles: one TMA producer, four
 //     splitter warps that split the streamed FP32 B tile (hi in place, lo in a
 //     sibling buffer), one MMA-issuing thread, four epilogue warps.  C arrives
 //     pre-split.  Two TMEM accumulators let an item's epilogue (U written
@@ -198,7 +200,7 @@ struct HalfCfg {
 };
 
 struct HalfParams {
-  int nao, naux, nocc, ldu, nitems, nqt, nk;
+  int nao, naux, nocc, ldq, nitems, nqt, nk, per_cta;
   float* u_hi;
   float* u_lo;
   double* rho;
@@ -252,8 +254,10 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
   if (warp == 0) {
     if (lane == 0) {  // producer
       int g = 0;
-      for (int item = blockIdx.x; item < p.nitems && !aborted(ctrl); item += gridDim.x) {
-        const int z = item / p.nqt, qt = item % p.nqt, mol = z / p.nao;
+      const int i0 = blockIdx.x * p.per_cta, i1 = min(p.nitems, i0 + p.per_cta);
+      for (int item = i0; item < i1 && !aborted(ctrl); ++item) {
+        const int mu = item % p.nao, qt = (item / p.nao) % p.nqt, mol = item / (p.nao * p.nqt);
+        const int z = mol * p.nao + mu;
         for (int kb = 0; kb < nk; ++kb, ++g) {
           const int s = g % S;
           if (g >= S && !mbar_wait(empty0 + 8 * s, ((g / S) - 1) & 1, ab)) {
@@ -272,7 +276,8 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
   } else if (warp >= 1 && warp <= 4) {  // splitters
     const int ts = tid - 32;
     int g = 0;
-    for (int item = blockIdx.x; item < p.nitems; item += gridDim.x) {
+    const int i0 = blockIdx.x * p.per_cta, i1 = min(p.nitems, i0 + p.per_cta);
+    for (int item = i0; item < i1; ++item) {
       for (int kb = 0; kb < nk; ++kb, ++g) {
         const int s = g % S;
         if (!mbar_wait(full0 + 8 * s, (g / S) & 1, ab)) {
@@ -299,7 +304,8 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
     if (lane == 0) {  // MMA issuer
       constexpr uint32_t idesc = instr_desc<BN>();
       int g = 0, t = 0;
-      for (int item = blockIdx.x; item < p.nitems && !aborted(ctrl); item += gridDim.x, ++t) {
+      const int i0 = blockIdx.x * p.per_cta, i1 = min(p.nitems, i0 + p.per_cta);
+      for (int item = i0; item < i1 && !aborted(ctrl); ++item, ++t) {
         const int b = t & 1;
         if (t >= 2 && !mbar_wait(ae0 + 8 * b, ((t >> 1) - 1) & 1, ab)) {
           set_abort(ctrl, p.error, 13);
@@ -336,19 +342,33 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
   } else {  // epilogue warps 6..9
     const int q = warp & 3;  // TMEM lane quarter this warp may access
     int t = 0;
-    for (int item = blockIdx.x; item < p.nitems; item += gridDim.x, ++t) {
+    const int i0 = blockIdx.x * p.per_cta, i1 = min(p.nitems, i0 + p.per_cta);
+    double rho_acc = 0.0;
+    int rho_key = -1;  // (mol, qt) whose rho rows rho_acc belongs to
+    for (int item = i0; item < i1; ++item, ++t) {
       const int b = t & 1;
+      const int mu = item % p.nao, key = item / p.nao;  // key = mol * nqt + qt
+      const int qt = key % p.nqt, mol = key / p.nqt;
+      const int z = mol * p.nao + mu;
+      const int row = qt * BM + q * 32 + lane;
+      const bool valid = row < p.naux;
+      if (key != rho_key) {
+        if (rho_key >= 0) {
+          const int prow = (rho_key % p.nqt) * BM + q * 32 + lane;
+          if (prow < p.naux && p.rho)
+            atomicAdd(p.rho + (size_t)(rho_key / p.nqt) * p.naux + prow, 2.0 * rho_acc);
+        }
+        rho_acc = 0.0;
+        rho_key = key;
+      }
       if (!mbar_wait(af0 + 8 * b, (t >> 1) & 1, ab)) {
         set_abort(ctrl, p.error, 15);
         break;
       }
       fence_after_sync();
-      const int z = item / p.nqt, qt = item % p.nqt;
-      const int row = qt * BM + q * 32 + lane;
-      const bool valid = row < p.naux;
-      double rho_part = 0.0;
-      float* uh = p.u_hi + ((size_t)z * p.naux + (valid ? row : 0)) * p.ldu;
-      float* ul = p.u_lo + ((size_t)z * p.naux + (valid ? row : 0)) * p.ldu;
+      // U[z][i][Q]: lanes run along Q, so every store is one coalesced 128-byte row
+      float* uh = p.u_hi + (size_t)z * p.nocc * p.ldq + row;
+      float* ul = p.u_lo + (size_t)z * p.nocc * p.ldq + row;
       const double* cv = p.cvec + (size_t)z * p.nocc;
 #pragma unroll
       for (int c = 0; c < BN; c += 16) {
@@ -358,19 +378,23 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
 #pragma unroll
           for (int k = 0; k < 16; ++k) {
             const int col = c + k;
-            if (col < p.ldu) {
+            if (col < p.nocc) {
               const float h = rn_tf32(v[k]);
-              uh[col] = h;
-              ul[col] = rn_tf32(v[k] - h);
+              uh[(size_t)col * p.ldq] = h;
+              ul[(size_t)col * p.ldq] = rn_tf32(v[k] - h);
+              rho_acc += (double)v[k] * __ldg(cv + col);
             }
-            if (col < p.nocc) rho_part += (double)v[k] * cv[col];
           }
         }
       }
       fence_before_sync();
       __syncwarp();
       if (lane == 0) mbar_arrive(ae0 + 8 * b);
-      if (valid && p.rho) atomicAdd(p.rho + (size_t)(z / p.nao) * p.naux + row, 2.0 * rho_part);
+    }
+    if (rho_key >= 0 && !aborted(ctrl)) {
+      const int prow = (rho_key % p.nqt) * BM + q * 32 + lane;
+      if (prow < p.naux && p.rho)
+        atomicAdd(p.rho + (size_t)(rho_key / p.nqt) * p.naux + prow, 2.0 * rho_acc);
     }
   }
 
@@ -654,7 +678,7 @@ static int launch_half(const CUtensorMap& ta, const CUtensorMap& th, const CUten
     if (e != cudaSuccess) return cuda_status(e, "half smem attribute");
     attr = true;
   }
-  const int grid = p.nitems < sm_count() ? p.nitems : sm_count();
+  const int grid = (p.nitems + p.per_cta - 1) / p.per_cta;
   half_ws_kernel<BN><<<grid, kHalfThreads, C::SMEM, st>>>(ta, th, tl, p);
   count_launch();
   return cuda_status(cudaGetLastError(), "half launch");
@@ -679,10 +703,11 @@ extern "C" int vqc_split_tf32(const float* x, float* hi, float* lo, int64_t n, v
 extern "C" int vqc_tc_half_transform(const float* b_aux_major, int32_t nmol, int32_t nao,
                                      int32_t ld_ao, int32_t naux, const float* ct_hi,
                                      const float* ct_lo, const double* c_occ, int32_t nocc,
-                                     int32_t o_pad, float* u_hi, float* u_lo, double* rho,
-                                     int32_t* error, void* stream) {
+                                     int32_t o_pad, int32_t ld_aux, float* u_hi, float* u_lo,
+                                     double* rho, int32_t* error, void* stream) {
   if (!b_aux_major || !ct_hi || !ct_lo || !c_occ || !u_hi || !u_lo || nmol <= 0 || nao <= 0 ||
-      naux <= 0 || nocc <= 0 || o_pad < nocc || o_pad % 16 || o_pad > 128 || ld_ao < nao)
+      naux <= 0 || nocc <= 0 || o_pad < nocc || o_pad % 16 || o_pad > 128 || ld_ao < nao ||
+      ld_aux < naux || ld_aux % 4)
     return fail(VQC_STATUS_INVALID_ARGUMENT, "half_transform: bad argument");
   CUtensorMap ta, th, tl;
   int st = make_map(&ta, b_aux_major, nao, ld_ao, naux, nmol * nao, BM);
@@ -693,11 +718,13 @@ extern "C" int vqc_tc_half_transform(const float* b_aux_major, int32_t nmol, int
   p.nao = nao;
   p.naux = naux;
   p.nocc = nocc;
-  p.ldu = o_pad;
+  p.ldq = ld_aux;
   p.nqt = (naux + BM - 1) / BM;
   const long long items = (long long)nmol * nao * p.nqt;
   if (items > 0x7fffffffLL) return fail(VQC_STATUS_INVALID_ARGUMENT, "half_transform: too many tiles");
   p.nitems = (int)items;
+  const int ctas = p.nitems < sm_count() ? p.nitems : sm_count();
+  p.per_cta = (p.nitems + ctas - 1) / ctas;
   p.nk = (nao + BK - 1) / BK;
   p.u_hi = u_hi;
   p.u_lo = u_lo;

@@ -92,8 +92,10 @@ class MixedBuilder:
         self.st = torch.cuda.current_stream().cuda_stream
         _lib.call("vqc_unpack_aux_major", b_packed.contiguous().data_ptr(), nb, n, x, self.ld,
                   self.b.data_ptr(), self.st)
-        self.u_hi = torch.empty(nb, n, x, self.o_pad, dtype=torch.float32, device=dev)
-        self.u_lo = torch.empty_like(self.u_hi)
+        # U[mol][mu][i][Q] split into TF32 hi/lo parts; Q rows padded to ldq
+        self.ldq = _round_up(x, 4)
+        self.u_hi = torch.zeros(nb, n, nocc, self.ldq, dtype=torch.float32, device=dev)
+        self.u_lo = torch.zeros_like(self.u_hi)
         self.rho = torch.empty(nb, x, dtype=torch.float64, device=dev)
         # the FP64 whitened rows stay resident for the refinement iterations,
         # the final energy and the gradient
@@ -119,7 +121,7 @@ class MixedBuilder:
         with TIMER.stage("K_half_tc"):
             self._lib.call("vqc_tc_half_transform", self.b.data_ptr(), nb, n, self.ld, self.x,
                            ct_hi.data_ptr(), ct_lo.data_ptr(), c64.data_ptr(), o, self.o_pad,
-                           self.u_hi.data_ptr(), self.u_lo.data_ptr(), self.rho.data_ptr(),
+                           self.ldq, self.u_hi.data_ptr(), self.u_lo.data_ptr(), self.rho.data_ptr(),
                            self.err.data_ptr(), self.st)
 
     def build(self, d: torch.Tensor, c_occ: torch.Tensor):
@@ -132,7 +134,7 @@ class MixedBuilder:
         k = torch.zeros(nb, n, n, dtype=torch.float64, device=d.device)
         with TIMER.stage("K_gram_tc"):
             self._lib.call("vqc_tc_gram", self.u_hi.data_ptr(), self.u_lo.data_ptr(), nb, n,
-                           self.x * self.o_pad, k.data_ptr(), self.err.data_ptr(), self.st)
+                           self.nocc * self.ldq, k.data_ptr(), self.err.data_ptr(), self.st)
         self.nbuild += 1
         self._check()
         return j, 2.0 * k

@@ -269,7 +269,7 @@ def _diis_extrapolate(errs: list, focks: list) -> torch.Tensor:
 def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision: str = "fp64",
             max_iterations: int = 100, energy_tolerance: float = 1e-10,
             density_tolerance: float = 1e-8, diis_history: int = 8,
-            relative_threshold: float = 1e-10) -> dict:
+            relative_threshold: float = 1e-10, trace: list | None = None) -> dict:
     """Batched SCF over one chunk; returns device tensors per molecule."""
     nb, n, x, nocc = chunk.nb, chunk.nao, chunk.naux, chunk.nocc
     dev = xyz.device
@@ -381,6 +381,10 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
             if bool((tight | ~active).all()) or phase_iterations >= MIXED_ITERATION_CAP:
                 phase, phase_iterations = "exact", 0
             done = torch.zeros_like(done)
+        if trace is not None:
+            trace.append((it, phase, float(de[active].max()) if bool(active.any()) else 0.0,
+                          float(cmax[active].max()) if bool(active.any()) else 0.0,
+                          int(active.sum())))
         newly = done & active
         # record the state of molecules that are still active
         final_e = torch.where(active, energy, final_e)
