@@ -65,7 +65,8 @@ def test_half_transform_and_gram(nb, n, x, o):
     uf = u.reshape(nb, n, kdim)
     kref = uf @ uf.transpose(1, 2)
     assert (k - kref).abs().max().item() <= 5e-6 * kref.abs().max().item()
-    assert torch.equal(k, k.transpose(1, 2)) or (k - k.transpose(1, 2)).abs().max() <= 1e-12 * kref.abs().max()
+    # off-diagonal tiles are mirrored exactly; diagonal tiles come from separate MMA lanes
+    assert (k - k.transpose(1, 2)).abs().max().item() <= 1e-9 * kref.abs().max().item()
 
 
 def test_split_tf32_exact_sum():

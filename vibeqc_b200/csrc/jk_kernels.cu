@@ -3,61 +3,66 @@
 // Reference: src/scf/cuda/df_coulomb.cpp:24 (packed cublasDgemv, FP64).
 //
 // HBM-streaming: one CTA per (molecule, mu) reads only the nu <= mu half of
-// B[mu] (J is symmetric), coalesced along nu, accumulates in FP64 with rho
-// staged in shared memory, and writes J[mu][nu] and its mirror J[nu][mu].
+// B[mu] (J is symmetric); its 8 warps split the Q range, lanes read float4
+// along nu, accumulate in FP64 with rho staged in shared memory, and the warp
+// partials are summed through shared memory into J[mu][nu] and J[nu][mu].
 #include "vqc_df.h"
 #include "vqc_plan.hpp"
 
 namespace vqc {
 
-constexpr int kJThreads = 128;
-constexpr int kJMaxNu = 4;  // nu per thread: N <= 512
+constexpr int kJThreads = 256;          // 8 warps share the Q range of one (mol, mu) row
+constexpr int kJWarps = kJThreads / 32;
+constexpr int kJMaxVec = 4;             // float4 per lane: nu < 4 * 32 * 4 = 512
 
 __global__ void __launch_bounds__(kJThreads)
     coulomb_fp32_kernel(const float* __restrict__ b, const double* __restrict__ rho, int n, int x,
                         int ld, double* __restrict__ j) {
-  extern __shared__ double srho[];
+  extern __shared__ double smem[];
+  double* srho = smem;                          // x
+  double* part = smem + ((x + 1) & ~1);         // kJWarps * ld partial sums
   const int mol = blockIdx.y, mu = blockIdx.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int q = threadIdx.x; q < x; q += kJThreads) srho[q] = rho[(size_t)mol * x + q];
   __syncthreads();
-  const float* row = b + ((size_t)mol * n + mu) * (size_t)x * ld;
-  double acc[kJMaxNu];
+  const float* rowb = b + ((size_t)mol * n + mu) * (size_t)x * ld;
+  const int nvec = (mu + 1 + 3) / 4;  // float4 columns covering nu <= mu (ld % 4 == 0)
+  double acc[kJMaxVec][4];
 #pragma unroll
-  for (int t = 0; t < kJMaxNu; ++t) acc[t] = 0.0;
-  const int nu_end = mu + 1;  // lower triangle nu <= mu
-  int q = 0;
-  for (; q + 4 <= x; q += 4) {
-    const double r0 = srho[q], r1 = srho[q + 1], r2 = srho[q + 2], r3 = srho[q + 3];
-    const float* p0 = row + (size_t)q * ld;
+  for (int t = 0; t < kJMaxVec; ++t)
 #pragma unroll
-    for (int t = 0; t < kJMaxNu; ++t) {
-      const int nu = threadIdx.x + t * kJThreads;
-      if (nu < nu_end) {
-        const float v0 = __ldg(p0 + nu), v1 = __ldg(p0 + ld + nu), v2 = __ldg(p0 + 2 * ld + nu),
-                    v3 = __ldg(p0 + 3 * ld + nu);
-        acc[t] = fma((double)v0, r0, acc[t]);
-        acc[t] = fma((double)v1, r1, acc[t]);
-        acc[t] = fma((double)v2, r2, acc[t]);
-        acc[t] = fma((double)v3, r3, acc[t]);
+    for (int e = 0; e < 4; ++e) acc[t][e] = 0.0;
+  for (int q = warp; q < x; q += kJWarps) {
+    const double r = srho[q];
+    const float4* p4 = reinterpret_cast<const float4*>(rowb + (size_t)q * ld);
+#pragma unroll
+    for (int t = 0; t < kJMaxVec; ++t) {
+      const int v = lane + 32 * t;
+      if (v < nvec) {
+        const float4 f = __ldg(p4 + v);
+        acc[t][0] = fma((double)f.x, r, acc[t][0]);
+        acc[t][1] = fma((double)f.y, r, acc[t][1]);
+        acc[t][2] = fma((double)f.z, r, acc[t][2]);
+        acc[t][3] = fma((double)f.w, r, acc[t][3]);
       }
     }
   }
-  for (; q < x; ++q) {
-    const double r = srho[q];
 #pragma unroll
-    for (int t = 0; t < kJMaxNu; ++t) {
-      const int nu = threadIdx.x + t * kJThreads;
-      if (nu < nu_end) acc[t] = fma((double)__ldg(row + (size_t)q * ld + nu), r, acc[t]);
+  for (int t = 0; t < kJMaxVec; ++t) {
+    const int v = lane + 32 * t;
+    if (v < nvec) {
+#pragma unroll
+      for (int e = 0; e < 4; ++e) part[warp * ld + 4 * v + e] = acc[t][e];
     }
   }
+  __syncthreads();
   double* jm = j + (size_t)mol * n * n;
+  for (int nu = threadIdx.x; nu <= mu; nu += kJThreads) {
+    double s = 0.0;
 #pragma unroll
-  for (int t = 0; t < kJMaxNu; ++t) {
-    const int nu = threadIdx.x + t * kJThreads;
-    if (nu < nu_end) {
-      jm[(size_t)mu * n + nu] = acc[t];
-      jm[(size_t)nu * n + mu] = acc[t];
-    }
+    for (int w = 0; w < kJWarps; ++w) s += part[w * ld + nu];
+    jm[(size_t)mu * n + nu] = s;
+    jm[(size_t)nu * n + mu] = s;
   }
 }
 
@@ -91,9 +96,10 @@ using namespace vqc;
 extern "C" int vqc_coulomb_fp32(const float* b_aux_major, const double* rho, int32_t nmol,
                                 int32_t nao, int32_t ld_ao, int32_t naux, double* j, void* stream) {
   if (!b_aux_major || !rho || !j || nmol <= 0 || nao <= 0 || naux <= 0 || ld_ao < nao ||
-      nao > kJThreads * kJMaxNu || nmol > 65535)
+      ld_ao % 4 || ld_ao > 4 * 32 * kJMaxVec || nmol > 65535 || nao > 65535)
     return fail(VQC_STATUS_INVALID_ARGUMENT, "coulomb_fp32: bad argument");
-  const size_t smem = (size_t)naux * sizeof(double);
+  const size_t smem = ((size_t)((naux + 1) & ~1) + (size_t)kJWarps * ld_ao) * sizeof(double);
+  if (smem > 200 * 1024) return fail(VQC_STATUS_INVALID_ARGUMENT, "coulomb_fp32: too many auxiliary functions");
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(coulomb_fp32_kernel,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
