@@ -348,7 +348,7 @@ class PreparedBatch:
 def _device_bytes_per_molecule(nao: int, naux: int, precision: str) -> int:
     """Peak device bytes one molecule holds during a chunk (integrals to gradient)."""
     p = nao * (nao + 1) // 2
-    per_px = 26 if precision == "fp64" else 28  # packed A/B + full B + packed Abar (+ FP32 B)
+    per_px = 26 if precision == "fp64" else 36  # packed A/B + full B + packed Abar (+ FP32 B)
     return int(per_px * p * naux + 64 * nao * nao)
 
 

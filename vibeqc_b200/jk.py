@@ -97,10 +97,10 @@ class MixedBuilder:
         self.u_hi = torch.zeros(nb, n, nocc, self.ldq, dtype=torch.float32, device=dev)
         self.u_lo = torch.zeros_like(self.u_hi)
         self.rho = torch.empty(nb, x, dtype=torch.float64, device=dev)
-        # the FP64 whitened rows stay resident for the refinement iterations,
-        # the final energy and the gradient
-        self.b_packed = b_packed
-        self.idx = unpack_index(n, dev)
+        # the FP64 whitened tensor stays resident (full rows, as on the FP64
+        # path) for the FP64 finishing iterations, the final energy and the
+        # gradient weights
+        self.b64 = b_packed[:, unpack_index(n, dev), :].contiguous()  # (nb, N*N, X)
         self.err = torch.zeros(1, dtype=torch.int32, device=dev)
         self.nbuild = 0
 
@@ -140,40 +140,37 @@ class MixedBuilder:
         return j, 2.0 * k
 
     def build_exact(self, d: torch.Tensor, c_occ: torch.Tensor):
-        """FP64 J and K from the FP64 whitened tensor (refinement phase)."""
+        """FP64 K and FP64-density J for the finishing iterations.
+
+        K = 2 U U^T with U = B C in FP64 from the FP64 tensor; J streams the
+        FP32 B with the exact fitted density (the energy reported at the end is
+        re-evaluated fully in FP64, so the FP32 storage of B in J only shifts
+        the converged density at second order in the energy).
+        """
         nb, n, x, o = self.nb, self.n, self.x, self.nocc
         rho, u = self.half_transform(c_occ)
-        with TIMER.stage("J_exact_fp64"):
-            j = torch.empty(nb, n, n, dtype=torch.float64, device=d.device)
-            for m in range(nb):
-                j[m] = (self._full64(m) @ rho[m]).view(n, n)
+        j = torch.empty(nb, n, n, dtype=torch.float64, device=d.device)
+        with TIMER.stage("J_fp32"):
+            self._lib.call("vqc_coulomb_fp32", self.b.data_ptr(), rho.data_ptr(), nb, n,
+                           self.ld, x, j.data_ptr(), self.st)
         with TIMER.stage("K_exact_fp64"):
             uf = u.reshape(nb, n, x * o)
             k = 2.0 * torch.bmm(uf, uf.transpose(1, 2))
         self.nbuild += 1
         return j, k
 
-    def _full64(self, m: int) -> torch.Tensor:
-        """(N*N, X) FP64 whitened rows of molecule m, unpacked on the fly."""
-        return self.b_packed[m][self.idx]
-
     def half_transform(self, c_occ: torch.Tensor):
         """FP64 (rho_whitened (nb, X), U (nb, N, X, o)) from the FP64 whitened tensor.
 
-        Used by the refinement iterations, the final energy and the gradient
+        Used by the finishing iterations, the final energy and the gradient
         weights, so the reported energy and forces carry no FP32 storage or
         tensor-core error.
         """
-        nb, n, x, o = self.nb, self.n, self.x, self.nocc
-        dev = c_occ.device
-        u = torch.empty(nb, n, x, o, dtype=torch.float64, device=dev)
-        rho = torch.empty(nb, x, dtype=torch.float64, device=dev)
+        nb, n, x = self.nb, self.n, self.x
         with TIMER.stage("exact_half_fp64"):
-            for m in range(nb):
-                b4 = self._full64(m).view(n, n, x)
-                u[m] = torch.matmul(b4.transpose(1, 2), c_occ[m])  # (mu, Q, i)
-                del b4
-                rho[m] = 2.0 * torch.einsum("mi,mqi->q", c_occ[m], u[m])
+            b4 = self.b64.view(nb, n, n, x)
+            u = torch.matmul(b4.transpose(2, 3), c_occ[:, None, :, :])  # (nb, N, X, o)
+            rho = 2.0 * torch.einsum("bmi,bmqi->bq", c_occ, u)
         return rho, u
 
 

@@ -103,6 +103,7 @@ class MetricFactor:
     rank: list
     condition: list                    # exact (eigen) or certified upper bound (Cholesky)
     kind: str = "eigen"
+    chol: torch.Tensor | None = None   # (nb, X, X) lower Cholesky factor (kind "cholesky")
 
 
 def factor_metric(metric: torch.Tensor, relative_threshold: float = 1e-10) -> MetricFactor:
@@ -131,7 +132,7 @@ def factor_metric(metric: torch.Tensor, relative_threshold: float = 1e-10) -> Me
             w = linv.transpose(1, 2).contiguous()
             keep = torch.ones(nb, x, dtype=torch.bool, device=m.device)
             cond = (lam_max_upper / lam_min_lower).tolist()
-            return MetricFactor(None, None, keep, w, [x] * nb, cond, "cholesky")
+            return MetricFactor(None, None, keep, w, [x] * nb, cond, "cholesky", l)
     lam, vec = torch.linalg.eigh(m)
     lmax = lam[:, -1:]
     keep = lam > relative_threshold * lmax
@@ -282,9 +283,13 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
         p_rows = b_packed.shape[1]
         blk = max(1024, (1 << 27) // (8 * x))  # ~128 MB temporaries
         for m in range(nb):
+            lt = mf.chol[m].transpose(0, 1) if mf.kind == "cholesky" else None
             for r0 in range(0, p_rows, blk):
                 rows = b_packed[m, r0:r0 + blk]
-                rows.copy_(rows @ mf.inv_sqrt[m])
+                if lt is not None:  # B = A L^-T by triangular solve: half the GEMM flops
+                    rows.copy_(torch.linalg.solve_triangular(lt, rows, upper=True, left=False))
+                else:
+                    rows.copy_(rows @ mf.inv_sqrt[m])
         jk = jkmod.make_builder(precision, b_packed, n, x, nocc)
         del b_packed
     s, h = ints.s, ints.h
@@ -305,9 +310,9 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
     gen.manual_seed(1234)
     guess = torch.randn(nb, n, nocc, dtype=torch.float64, device=dev, generator=gen)
 
-    def density_from(f, guess):
+    def density_from(f, guess, tol=1e-11):
         with TIMER.stage("purify"):
-            proj = purify_sp2(xo.transpose(1, 2) @ f @ xo, nocc)
+            proj = purify_sp2(xo.transpose(1, 2) @ f @ xo, nocc, tol=tol)
             co = occupied_factor(proj, guess, gen)  # orthonormal, orthogonal basis
         return 2.0 * (xo @ proj @ xo.transpose(1, 2)), co
 
@@ -354,7 +359,8 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
         errs, focks = errs[-diis_history:], focks[-diis_history:]
         f_ext = _diis_extrapolate(errs, focks) if len(errs) > 1 else f
         TIMER_ctx.__exit__(None, None, None)
-        d_new, co = density_from(f_ext, co)
+        # the tensor-core phase only needs the projector to its own accuracy
+        d_new, co = density_from(f_ext, co, 1e-11 if phase == "exact" else 1e-8)
         TIMER_ctx = TIMER.stage("scf_other")
         TIMER_ctx.__enter__()
         c_new = xo @ co
