@@ -283,13 +283,9 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
         p_rows = b_packed.shape[1]
         blk = max(1024, (1 << 27) // (8 * x))  # ~128 MB temporaries
         for m in range(nb):
-            lt = mf.chol[m].transpose(0, 1) if mf.kind == "cholesky" else None
             for r0 in range(0, p_rows, blk):
                 rows = b_packed[m, r0:r0 + blk]
-                if lt is not None:  # B = A L^-T by triangular solve: half the GEMM flops
-                    rows.copy_(torch.linalg.solve_triangular(lt, rows, upper=True, left=False))
-                else:
-                    rows.copy_(rows @ mf.inv_sqrt[m])
+                rows.copy_(rows @ mf.inv_sqrt[m])  # GEMM: measured faster than DTRSM here
         jk = jkmod.make_builder(precision, b_packed, n, x, nocc)
         del b_packed
     s, h = ints.s, ints.h
