@@ -185,6 +185,8 @@ class PreparedBatch:
         self._calc = calculator
         self._closed = False
         self._warm_start = warm_start
+        self.charges = tuple(int(q) for q in charges)
+        self.multiplicities = tuple(int(m) for m in mults)
         self._molecules = []
         for atoms, q, m in zip(systems, charges, mults):
             mol = make_molecule(atoms, calculator.basis, calculator.auxiliary_basis, q, m)
@@ -211,6 +213,7 @@ class PreparedBatch:
                 self._chunks.append(Chunk([self._molecules[i] for i in part], part,
                                           calculator.spherical))
         self._natoms = [len(m.atomic_numbers) for m in self._molecules]
+        self.atomic_numbers = tuple(tuple(int(z) for z in m.atomic_numbers) for m in self._molecules)
 
     @property
     def size(self) -> int:
@@ -283,6 +286,39 @@ class PreparedBatch:
         """
         with torch.cuda.device(self._calc.device):
             return [self._run_chunk(c, x, want_forces) for c, x in zip(self._chunks, xyz_chunks)]
+
+    def execute_tensors(self, coordinates: list) -> tuple:
+        """Energies and gradients for per-system coordinate tensors, on the device.
+
+        Returns ``(energies (nsys,) FP64, [dE/dR (natoms, 3) FP64 per system])``
+        on the calculator's device; raises if any system fails or does not
+        converge (the autograd path needs every value).
+        """
+        if self._closed:
+            raise RuntimeError("prepared batch is closed")
+        if len(coordinates) != len(self._molecules):
+            raise ValueError("coordinates must give one tensor per system")
+        dev = self._calc.device
+        energies = torch.empty(len(self._molecules), dtype=torch.float64, device=dev)
+        grads: list = [None] * len(self._molecules)
+        with torch.cuda.device(dev):
+            for chunk in self._chunks:
+                parts = []
+                for i in chunk.indices:
+                    c = coordinates[i].to(device=dev, dtype=torch.float64)
+                    if tuple(c.shape) != (self._natoms[i], 3) or not bool(torch.isfinite(c).all()):
+                        raise ValueError(f"system {i}: coordinates must be finite ({self._natoms[i]}, 3)")
+                    parts.append(c)
+                xyz = torch.cat(parts, dim=0).contiguous()
+                out, g = self._run_chunk(chunk, xyz, True)
+                if not bool(out["converged"].all()):
+                    raise RuntimeError("SCF did not converge for a system of the batch")
+                off = 0
+                for j, i in enumerate(chunk.indices):
+                    energies[i] = out["energy"][j]
+                    grads[i] = g[off:off + self._natoms[i]]
+                    off += self._natoms[i]
+        return energies, grads
 
     def execute(self, coordinates=None, *, strict: bool = False,
                 properties: Iterable[str] | None = None) -> BatchResult:
