@@ -129,6 +129,13 @@ def algorithmic_model(batch) -> dict:
             "grad3c_bytes": bytes_grad3c}
 
 
+def max_over_ranks(v: float) -> float:
+    from vibeqc_b200.distributed import max_over_ranks as _m
+    import torch
+
+    return _m(v, torch.device("cuda", torch.cuda.current_device()) if torch.cuda.is_available() else None)
+
+
 def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     import torch
 
@@ -149,15 +156,6 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
             import torch.distributed as dist
 
             dist.barrier()
-
-    def max_over_ranks(v: float) -> float:
-        if world == 1:
-            return v
-        import torch.distributed as dist
-
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
 
     for _ in range(args.warmup):
         outs = batch.execute_device(xyz)
@@ -202,6 +200,34 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
 
     model = algorithmic_model(batch)
     steps = args.steps
+
+    compare = None
+    if args.precision == "mixed" and not args.no_compare:
+        # FP64 GPU plan of the same molecules: throughput (one warm-up, one
+        # timed step, device-resident) and per-molecule |dE|, max|dF|
+        calc64 = Calculator(method="rhf", basis=BASIS, auxiliary_basis=AUX, device="cuda",
+                            device_id=local_rank, density_fitting="cuda", precision="fp64")
+        b64 = calc64.prepare_batch(systems)
+        x64 = b64.upload_coordinates()
+        warm = b64.execute_device(x64)
+        del warm
+        torch.cuda.synchronize()
+        s64, e64 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s64.record()
+        outs64 = b64.execute_device(x64)
+        e64.record()
+        torch.cuda.synchronize()
+        ms64 = max_over_ranks(s64.elapsed_time(e64))
+        value64 = args.count * world / (ms64 / 1000.0)
+        r64 = b64.execute(coords_host)
+        del outs64
+        de = max(abs(a.energy - b.energy) for a, b in zip(res.items, r64.items))
+        df = max(float(np.abs(a.forces - b.forces).max()) for a, b in zip(res.items, r64.items))
+        compare = {"fp64_gpu_value": round(value64, 3), "fp64_gpu_ms_per_step": round(ms64, 1),
+                   "speedup_vs_fp64_gpu": round(value / value64, 3), "max_abs_dE_Eh": de,
+                   "max_abs_dF_Eh_per_bohr": df,
+                   "within_target": bool(de <= 1e-6 and df <= 1e-5)}
+        b64.close()
     rl = None
     if "int3c" in stages:
         t_int3c = stages["int3c"]["ms"] / 1000.0 / steps
@@ -248,6 +274,16 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         "roofline": rl,
         "stages_ms_per_step": {k: round(v["ms"] / steps, 3) for k, v in stages.items()},
     }
+    if compare is not None:
+        out["mixed_vs_fp64"] = compare
+    if "K_gram_tc" in stages:
+        t_k = (stages["K_gram_tc"]["ms"] + stages["K_half_tc"]["ms"]) / 1000.0 / steps
+        builds = stages["K_gram_tc"]["launch_groups"] / steps / max(len(batch._chunks), 1)
+        out["k_tflops"] = round(model["k_flops_per_build"] * builds / t_k / 1e12, 2)
+    elif "K_fp64" in stages:
+        t_k = stages["K_fp64"]["ms"] / 1000.0 / steps
+        builds = stages["K_fp64"]["launch_groups"] / steps / max(len(batch._chunks), 1)
+        out["k_tflops"] = round(model["k_flops_per_build"] * builds / t_k / 1e12, 2)
     batch.close()
     return out
 
@@ -266,7 +302,9 @@ def main() -> int:
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--precision", choices=["mixed", "fp64"], default="fp64")
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--no-compare", action="store_true",
+                    help="skip the FP64 GPU comparator run (energies/forces/throughput)")
     ap.add_argument("--count", type=int, default=256)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -153,6 +153,9 @@ int vqc_sp2_update(const double* x, const double* x2, double* xout, int32_t nmol
  *     U (3xTF32, FP64 output); reference df_occupied_exchange.cpp:262-279.
  *   vqc_coulomb_fp32: J[mol][mu][nu] = sum_Q B[mu][Q][nu] rho[mol][Q] (FP64
  *     accumulate); reference src/scf/cuda/df_coulomb.cpp:24.
+ *   vqc_fitted_density_fp32: rho[mol][Q] = sum_{mu,nu} B[mu][Q][nu] D[mu][nu]
+ *     for symmetric D [mol][nao][nao] (FP64 accumulate); reference
+ *     df_coulomb.cpp:38-57.
  * error: device int set non-zero when a bounded wait inside a tensor-core
  * kernel expires (the kernel then stops early; the caller must treat the
  * output as invalid).
@@ -168,6 +171,8 @@ int vqc_tc_gram(const float* u_hi, const float* u_lo, int32_t nmol, int32_t nao,
                 double* kout, int32_t* error, void* stream);
 int vqc_coulomb_fp32(const float* b_aux_major, const double* rho, int32_t nmol, int32_t nao,
                      int32_t ld_ao, int32_t naux, double* j, void* stream);
+int vqc_fitted_density_fp32(const float* b_aux_major, const double* dens, int32_t nmol,
+                            int32_t nao, int32_t ld_ao, int32_t naux, double* rho, void* stream);
 
 #ifdef __cplusplus
 }

@@ -97,6 +97,24 @@ def test_coulomb_fp32(nb, n, x):
     assert (j - ref).abs().max().item() <= 1e-12 * ref.abs().max().item() * x**0.5
 
 
+@pytest.mark.parametrize("nb,n,x", [(2, 40, 200), (1, 384, 1856), (3, 13, 77)])
+def test_fitted_density_fp32(nb, n, x):
+    ld = (n + 3) // 4 * 4
+    g = torch.Generator(device="cuda").manual_seed(4)
+    full = torch.randn(nb, n, n, x, generator=g, device="cuda", dtype=torch.float64)
+    full = 0.5 * (full + full.transpose(1, 2))
+    b = torch.zeros(nb, n, x, ld, dtype=torch.float32, device="cuda")
+    b[..., :n] = full.permute(0, 1, 3, 2).float()
+    d = torch.randn(nb, n, n, generator=g, device="cuda", dtype=torch.float64)
+    d = 0.5 * (d + d.transpose(1, 2))
+    rho = torch.full((nb, x), float("nan"), dtype=torch.float64, device="cuda")
+    _lib.call("vqc_fitted_density_fp32", b.data_ptr(), d.data_ptr(), nb, n, ld, x, rho.data_ptr(),
+              torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    ref = torch.einsum("bmqn,bmn->bq", b[..., :n].double(), d)
+    assert (rho - ref).abs().max().item() <= 1e-12 * ref.abs().max().item() * n
+
+
 def test_unpack_aux_major_roundtrip():
     nb, n, x = 2, 11, 37
     ld = 12

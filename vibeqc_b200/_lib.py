@@ -96,6 +96,8 @@ _SIGNATURES = {
                                ctypes.c_int32, _P, _P, _P, _P, _P], ctypes.c_int),
     "vqc_tc_gram": ([_P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _P, _P, _P],
                     ctypes.c_int),
+    "vqc_fitted_density_fp32": ([_P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                 ctypes.c_int32, _P, _P], ctypes.c_int),
     "vqc_coulomb_fp32": ([_P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                           ctypes.c_int32, _P, _P], ctypes.c_int),
 }

@@ -382,7 +382,7 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
               const float h = rn_tf32(v[k]);
               uh[(size_t)col * p.ldq] = h;
               ul[(size_t)col * p.ldq] = rn_tf32(v[k] - h);
-              rho_acc += (double)v[k] * __ldg(cv + col);
+              if (p.rho) rho_acc += (double)v[k] * __ldg(cv + col);
             }
           }
         }

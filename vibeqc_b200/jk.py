@@ -8,8 +8,9 @@ as in ``src/scf/cuda/df_occupied_exchange.cpp:191-300``.
 ``mixed``: B stored once in FP32 (aux-major per AO row); the exchange half
 transform U = B C and the Gram product K = 2 U U^T run on the tcgen05 tensor
 cores in split precision (3xTF32: round-to-nearest hi/lo parts, FP32
-accumulation drained to FP64), the fitted density rho comes out of the half
-transform's epilogue, and J streams the FP32 B once with FP64 accumulation.
+accumulation drained to FP64); the fitted density rho = B^T d and J = B rho
+stream the FP32 B with FP64 accumulation.  The FP64 tensor stays resident for
+the finishing iterations, the final energy and the gradient.
 """
 
 from __future__ import annotations
@@ -117,11 +118,10 @@ class MixedBuilder:
         self._lib.call("vqc_split_tf32", ct.data_ptr(), ct_hi.data_ptr(), ct_lo.data_ptr(),
                        ct.numel(), self.st)
         c64 = c_occ.contiguous()
-        self.rho.zero_()
         with TIMER.stage("K_half_tc"):
             self._lib.call("vqc_tc_half_transform", self.b.data_ptr(), nb, n, self.ld, self.x,
                            ct_hi.data_ptr(), ct_lo.data_ptr(), c64.data_ptr(), o, self.o_pad,
-                           self.ldq, self.u_hi.data_ptr(), self.u_lo.data_ptr(), self.rho.data_ptr(),
+                           self.ldq, self.u_hi.data_ptr(), self.u_lo.data_ptr(), 0,
                            self.err.data_ptr(), self.st)
 
     def build(self, d: torch.Tensor, c_occ: torch.Tensor):
@@ -129,6 +129,11 @@ class MixedBuilder:
         self._half(c_occ)
         j = torch.empty(nb, n, n, dtype=torch.float64, device=d.device)
         with TIMER.stage("J_fp32"):
+            # fitted density from the FP32 B with FP64 accumulation (no
+            # tensor-core accumulation error in J), then J = B rho
+            dd = d.contiguous()
+            self._lib.call("vqc_fitted_density_fp32", self.b.data_ptr(), dd.data_ptr(), nb, n,
+                           self.ld, self.x, self.rho.data_ptr(), self.st)
             self._lib.call("vqc_coulomb_fp32", self.b.data_ptr(), self.rho.data_ptr(), nb, n,
                            self.ld, self.x, j.data_ptr(), self.st)
         k = torch.zeros(nb, n, n, dtype=torch.float64, device=d.device)
