@@ -151,11 +151,21 @@ int vqc_sp2_update(const double* x, const double* x2, double* xout, int32_t nmol
  *     Reference src/scf/cuda/df_occupied_exchange.cpp:251-257 (U = B C).
  *   vqc_tc_gram: kout[mol] += U U^T over kdim = nocc * ld_aux from the split
  *     U (3xTF32, FP64 output); reference df_occupied_exchange.cpp:262-279.
+ *   vqc_tc_gram_sym2: kout[mol] += A B^T + B A^T for two split operands of
+ *     the same layout; forms the incremental exchange about an FP64 anchor,
+ *     K(D) = K(D0) + 2 (V dU^T + dU V^T) with dU = B (C - C0) and
+ *     V = U0 + dU / 2 (no counterpart in the reference, which rebuilds K in
+ *     FP64 every iteration).
  *   vqc_coulomb_fp32: J[mol][mu][nu] = sum_Q B[mu][Q][nu] rho[mol][Q] (FP64
  *     accumulate); reference src/scf/cuda/df_coulomb.cpp:24.
  *   vqc_fitted_density_fp32: rho[mol][Q] = sum_{mu,nu} B[mu][Q][nu] D[mu][nu]
  *     for symmetric D [mol][nao][nao] (FP64 accumulate); reference
  *     df_coulomb.cpp:38-57.
+ *   vqc_anchor_combine: with the FP64 anchor u0[rows][x] and the split
+ *     increment du_hi/du_lo[rows][ld_aux]: mode 0 writes the split
+ *     V = u0 + alpha (du_hi + du_lo) into v_hi/v_lo[rows][ld_aux] (padding
+ *     zero); mode 1 adds alpha (du_hi + du_lo) into u0 in place.  No
+ *     counterpart in the reference.
  * error: device int set non-zero when a bounded wait inside a tensor-core
  * kernel expires (the kernel then stops early; the caller must treat the
  * output as invalid).
@@ -169,6 +179,12 @@ int vqc_tc_half_transform(const float* b_aux_major, int32_t nmol, int32_t nao, i
                           float* u_hi, float* u_lo, double* rho, int32_t* error, void* stream);
 int vqc_tc_gram(const float* u_hi, const float* u_lo, int32_t nmol, int32_t nao, int32_t kdim,
                 double* kout, int32_t* error, void* stream);
+int vqc_tc_gram_sym2(const float* a_hi, const float* a_lo, const float* b_hi, const float* b_lo,
+                     int32_t nmol, int32_t nao, int32_t kdim, double* kout, int32_t* error,
+                     void* stream);
+int vqc_anchor_combine(double* u0, const float* du_hi, const float* du_lo, float* v_hi,
+                       float* v_lo, int64_t rows, int32_t x, int32_t ld_aux, double alpha,
+                       int32_t mode, void* stream);
 int vqc_coulomb_fp32(const float* b_aux_major, const double* rho, int32_t nmol, int32_t nao,
                      int32_t ld_ao, int32_t naux, double* j, void* stream);
 int vqc_fitted_density_fp32(const float* b_aux_major, const double* dens, int32_t nmol,

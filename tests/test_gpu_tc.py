@@ -69,6 +69,62 @@ def test_half_transform_and_gram(nb, n, x, o):
     assert (k - k.transpose(1, 2)).abs().max().item() <= 1e-9 * kref.abs().max().item()
 
 
+def _split(t):
+    hi, lo = torch.empty_like(t), torch.empty_like(t)
+    _lib.call("vqc_split_tf32", t.data_ptr(), hi.data_ptr(), lo.data_ptr(), t.numel(),
+              torch.cuda.current_stream().cuda_stream)
+    return hi, lo
+
+
+@pytest.mark.parametrize("nb,n,kdim", [(2, 40, 256), (1, 200, 1040), (3, 130, 4000)])
+def test_gram_sym2_matches_fp64(nb, n, kdim):
+    """kout += A B^T + B A^T on top of an existing FP64 value (the anchor K0 / 2)."""
+    g = torch.Generator(device="cuda").manual_seed(11)
+    a = torch.randn(nb, n, kdim, generator=g, device="cuda", dtype=torch.float32)
+    b = 1e-3 * torch.randn(nb, n, kdim, generator=g, device="cuda", dtype=torch.float32)
+    ah, al = _split(a)
+    bh, bl = _split(b)
+    base = torch.randn(nb, n, n, generator=g, device="cuda", dtype=torch.float64)
+    base = base + base.transpose(1, 2)
+    k = base.clone()
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    _lib.call("vqc_tc_gram_sym2", ah.data_ptr(), al.data_ptr(), bh.data_ptr(), bl.data_ptr(), nb, n,
+              kdim, k.data_ptr(), err.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    a64, b64 = (ah.double() + al.double()), (bh.double() + bl.double())
+    inc = a64 @ b64.transpose(1, 2) + b64 @ a64.transpose(1, 2)
+    got = k - base
+    # the increment's error scales with |A| |B|, not with the base value
+    assert (got - inc).abs().max().item() <= 5e-6 * inc.abs().max().item()
+    assert (k - k.transpose(1, 2)).abs().max().item() <= 1e-9 * inc.abs().max().item() + 1e-12
+
+
+def test_anchor_combine_modes():
+    g = torch.Generator(device="cuda").manual_seed(5)
+    rows, x, ldq = 777, 130, 132
+    u0 = torch.randn(rows, x, generator=g, device="cuda", dtype=torch.float64)
+    du = torch.zeros(rows, ldq, device="cuda", dtype=torch.float32)
+    du[:, :x] = 1e-4 * torch.randn(rows, x, generator=g, device="cuda")
+    dh, dl = _split(du)
+    vh = torch.full((rows, ldq), 7.0, device="cuda", dtype=torch.float32)
+    vl = torch.full_like(vh, 7.0)
+    st = torch.cuda.current_stream().cuda_stream
+    _lib.call("vqc_anchor_combine", u0.data_ptr(), dh.data_ptr(), dl.data_ptr(), vh.data_ptr(),
+              vl.data_ptr(), rows, x, ldq, 0.5, 0, st)
+    torch.cuda.synchronize()
+    want = u0 + 0.5 * (dh[:, :x].double() + dl[:, :x].double())
+    got = vh[:, :x].double() + vl[:, :x].double()
+    assert ((vh.view(torch.int32) & 0x1FFF) == 0).all()
+    assert (got - want).abs().max().item() <= 2.0**-21 * want.abs().max().item()
+    assert (vh[:, x:] == 0).all() and (vl[:, x:] == 0).all()
+    ref = u0 + (dh[:, :x].double() + dl[:, :x].double())
+    _lib.call("vqc_anchor_combine", u0.data_ptr(), dh.data_ptr(), dl.data_ptr(), 0, 0, rows, x,
+              ldq, 1.0, 1, st)
+    torch.cuda.synchronize()
+    assert (u0 - ref).abs().max().item() <= 1e-15 * ref.abs().max().item()
+
+
 def test_split_tf32_exact_sum():
     x = torch.randn(10007, device="cuda", dtype=torch.float32) * 1e3
     hi, lo = torch.empty_like(x), torch.empty_like(x)

@@ -1,0 +1,102 @@
+"""Host-side FP64 linear algebra of the SCF driver, checked on the CPU."""
+
+import numpy as np
+import pytest
+import torch
+
+from vibeqc_b200 import scf
+
+
+def _spd(nb, x, cond, seed):
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(nb):
+        q, _ = np.linalg.qr(rng.standard_normal((x, x)))
+        lam = np.geomspace(1.0, 1.0 / cond, x)
+        out.append((q * lam) @ q.T)
+    return torch.tensor(np.array(out))
+
+
+@pytest.mark.parametrize("x,p", [(37, 50), (300, 700), (513, 129)])
+def test_whiten_in_place_matches_dense_product(x, p, monkeypatch):
+    monkeypatch.setattr(scf, "WHITEN_COLUMN_BLOCK", 64)
+    m = _spd(2, x, 1e5, x)
+    mf = scf.factor_metric(m)
+    assert mf.kind == "cholesky"
+    a = torch.randn(2, p, x, dtype=torch.float64, generator=torch.Generator().manual_seed(3))
+    ref = a @ mf.inv_sqrt
+    scf.whiten_in_place(a, mf)
+    assert torch.allclose(a, ref, rtol=0, atol=1e-12 * ref.abs().max().item())
+    # W W^T = M^-1
+    ww = mf.inv_sqrt @ mf.inv_sqrt.transpose(1, 2)
+    assert torch.allclose(ww @ m, torch.eye(x, dtype=torch.float64).expand(2, x, x), atol=1e-6)
+
+
+def test_whiten_eigen_factor_dense():
+    m = _spd(1, 40, 1e14, 1)  # cutoff active -> eigen factor with reduced rank
+    mf = scf.factor_metric(m, relative_threshold=1e-10)
+    assert mf.kind == "eigen" and mf.rank[0] < 40
+    a = torch.randn(1, 60, 40, dtype=torch.float64)
+    ref = a @ mf.inv_sqrt
+    scf.whiten_in_place(a, mf)
+    assert torch.allclose(a, ref, rtol=0, atol=1e-12 * ref.abs().max().item())
+
+
+def test_occupied_factor_without_noise_stays_aligned():
+    g = torch.Generator().manual_seed(0)
+    n, o = 30, 6
+    q, _ = torch.linalg.qr(torch.randn(1, n, n, dtype=torch.float64, generator=g))
+    c0 = q[:, :, :o]
+    # a slightly rotated occupied space
+    k = 1e-4 * torch.randn(1, n - o, o, dtype=torch.float64, generator=g)
+    c1 = c0 + q[:, :, o:] @ k
+    c1, _ = torch.linalg.qr(c1)
+    proj = c1 @ c1.transpose(1, 2)
+    co = scf.occupied_factor(proj, c0, g, noise_scale=0.0)
+    assert torch.allclose(co.transpose(1, 2) @ co, torch.eye(o, dtype=torch.float64)[None], atol=1e-12)
+    assert torch.allclose(co @ co.transpose(1, 2), proj, atol=1e-12)
+    assert (co - c0).abs().max().item() < 1e-3  # aligned to the guess, O(|rotation|)
+
+
+@pytest.mark.parametrize("n,o,x,upper", [(13, 3, 40, True), (70, 9, 300, True), (45, 6, 100, False)])
+def test_gradient_weights_match_dense_formulas(n, o, x, upper, monkeypatch):
+    from vibeqc_b200 import gradient as gr
+
+    monkeypatch.setattr(gr, "WEIGHT_ROW_BLOCK", 8)
+    monkeypatch.setattr(gr, "SYM_BLOCK", 64)
+    g = torch.Generator().manual_seed(n)
+    c = torch.randn(n, o, dtype=torch.float64, generator=g)
+    dens = 2.0 * c @ c.T
+    rho = torch.randn(x, dtype=torch.float64, generator=g)
+    u = torch.randn(n, o, x, dtype=torch.float64, generator=g)
+    w = torch.randn(x, x, dtype=torch.float64, generator=g)
+    if upper:
+        w = torch.triu(w)
+    abar, mbar = gr.molecule_weights(c, dens, rho, u, w, upper)
+    # dense restatement: Abar = D (x) cvec - 2 C Gamma C^T, Mbar = -cc^T/2 + Gamma Gamma^T
+    cvec = w @ rho
+    bij = torch.einsum("mi,mjq->qij", c, u)
+    gam = (w @ bij.reshape(x, o * o)).view(x, o, o)
+    full = dens[:, :, None] * cvec - 2.0 * torch.einsum("mi,nj,pij->mnp", c, c, gam)
+    mu, nu = torch.tril_indices(n, n)
+    ref_abar = full[mu, nu]
+    ref_mbar = -0.5 * torch.outer(cvec, cvec) + gam.reshape(x, -1) @ gam.reshape(x, -1).T
+    assert torch.allclose(abar, ref_abar, rtol=0, atol=1e-11 * ref_abar.abs().max().item())
+    assert torch.allclose(mbar, ref_mbar, rtol=0, atol=1e-11 * ref_mbar.abs().max().item())
+
+
+def test_packed_half_transform_matches_full(monkeypatch):
+    from vibeqc_b200 import jk
+
+    monkeypatch.setattr(jk, "HALF_BLOCK_BYTES", 8 * 3 * 11 * 17 * 2)  # two AO rows per block
+    g = torch.Generator().manual_seed(2)
+    nb, n, x, o = 3, 11, 17, 4
+    bp = torch.randn(nb, n * (n + 1) // 2, x, dtype=torch.float64, generator=g)
+    c = torch.randn(nb, n, o, dtype=torch.float64, generator=g)
+    full = bp[:, jk.unpack_index(n, "cpu")].view(nb, n, n, x)
+    rho, u = jk.fp64_half_packed(bp, c, n, x)
+    rho_f, u_f = jk.fp64_half(full.reshape(nb, n * n, x), c, n, x)
+    ref = torch.einsum("bmnq,bni->bmiq", full, c)
+    assert torch.allclose(u, ref, atol=1e-12) and torch.allclose(u_f, ref, atol=1e-12)
+    assert torch.allclose(rho, rho_f, atol=1e-11)
+    assert torch.allclose(rho, torch.einsum("bmnq,bmn->bq", full, 2 * c @ c.transpose(1, 2)), atol=1e-10)

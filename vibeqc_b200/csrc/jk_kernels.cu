@@ -137,9 +137,62 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// Incremental exchange about an FP64 anchor U0 = B C0 ([row][Q], rows of
+// length x) and the tensor-core increment dU = B (C - C0) (split hi/lo, rows
+// of length ldq):
+//   mode 0: V = U0 + alpha (dU_hi + dU_lo), written split into v_hi / v_lo
+//           (round-to-nearest TF32 parts, padding columns zero);
+//   mode 1: U0 += alpha (dU_hi + dU_lo) in place (FP64).
+__global__ void __launch_bounds__(256)
+    anchor_combine_kernel(double* __restrict__ u0, const float* __restrict__ du_hi,
+                          const float* __restrict__ du_lo, float* __restrict__ v_hi,
+                          float* __restrict__ v_lo, long long rows, int x, int ldq, double alpha,
+                          int mode) {
+  const long long total = rows * (long long)ldq;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long r = e / ldq;
+    const int q = (int)(e - r * ldq);
+    if (q >= x) {
+      if (mode == 0) {
+        v_hi[e] = 0.0f;
+        v_lo[e] = 0.0f;
+      }
+      continue;
+    }
+    const double d = (double)__ldg(du_hi + e) + (double)__ldg(du_lo + e);
+    double* p = u0 + r * x + q;
+    if (mode == 1) {
+      *p += alpha * d;
+    } else {
+      const float v = (float)(*p + alpha * d);
+      uint32_t hb, lb;
+      asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hb) : "f"(v));
+      const float h = __uint_as_float(hb);
+      asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lb) : "f"(v - h));
+      v_hi[e] = h;
+      v_lo[e] = __uint_as_float(lb);
+    }
+  }
+}
+
 }  // namespace vqc
 
 using namespace vqc;
+
+extern "C" int vqc_anchor_combine(double* u0, const float* du_hi, const float* du_lo, float* v_hi,
+                                  float* v_lo, int64_t rows, int32_t x, int32_t ld_aux,
+                                  double alpha, int32_t mode, void* stream) {
+  if (!u0 || !du_hi || !du_lo || rows <= 0 || x <= 0 || ld_aux < x || (mode != 0 && mode != 1) ||
+      (mode == 0 && (!v_hi || !v_lo)))
+    return fail(VQC_STATUS_INVALID_ARGUMENT, "anchor_combine: bad argument");
+  long long blocks = (rows * (long long)ld_aux + 255) / 256;
+  blocks = blocks > 8 * 148 ? 8 * 148 : blocks;
+  anchor_combine_kernel<<<(int)blocks, 256, 0, (cudaStream_t)stream>>>(
+      u0, du_hi, du_lo, v_hi, v_lo, (long long)rows, x, ld_aux, alpha, mode);
+  count_launch();
+  return cuda_status(cudaGetLastError(), "anchor_combine");
+}
 
 extern "C" int vqc_coulomb_fp32(const float* b_aux_major, const double* rho, int32_t nmol,
                                 int32_t nao, int32_t ld_ao, int32_t naux, double* j, void* stream) {

@@ -20,7 +20,9 @@
 //   gram_ws_kernel -- K[mol] += U U^T over kdim = X * o_pad (reference
 //     df_occupied_exchange.cpp:262-279) from the pre-split U: a pure
 //     TMA -> MMA pipeline over upper-triangle 128x128 tiles and split K
-//     ranges.  The tensor core's FP32 accumulation is not round-to-nearest
+//     ranges.  The symmetric two-operand form K += A B^T + B A^T (two K
+//     segments, operands swapped in the second) serves the incremental
+//     exchange K(D) = K(D0) + 2 (V dU^T + dU V^T) about an FP64 anchor.  The tensor core's FP32 accumulation is not round-to-nearest
 //     (about 2^-24 relative bias per accumulation step), so chains are kept to
 //     kGramFlush K-blocks and drained into FP64 registers by eight epilogue
 //     warps (double-buffered TMEM); tiles add FP64 partials (and the mirror
@@ -438,12 +440,14 @@ struct GramCfg {
 
 struct GramParams {
   int nao, kdim, ntiles_ut, nt, kblocks_per_split, ksplit;
+  int nseg;  // 1: A A^T (B maps unused); 2: A B^T + B A^T
   double* kout;
   int* error;
 };
 
 __global__ void __launch_bounds__(kGramThreads, 1)
-    gram_ws_kernel(const __grid_constant__ CUtensorMap tmH, const __grid_constant__ CUtensorMap tmL,
+    gram_ws_kernel(const __grid_constant__ CUtensorMap tmAH, const __grid_constant__ CUtensorMap tmAL,
+                   const __grid_constant__ CUtensorMap tmBH, const __grid_constant__ CUtensorMap tmBL,
                    GramParams p) {
   using C = GramCfg;
   constexpr int S = C::S;
@@ -462,7 +466,8 @@ __global__ void __launch_bounds__(kGramThreads, 1)
   }
   const int nt = mt + rem;
   const int z = blockIdx.y / p.ksplit, split = blockIdx.y % p.ksplit;
-  const int kb_total = (p.kdim + BK - 1) / BK;
+  const int kb_seg = (p.kdim + BK - 1) / BK;  // K-blocks per segment
+  const int kb_total = kb_seg * p.nseg;
   const int kb0 = split * p.kblocks_per_split;
   const int kb1 = min(kb_total, kb0 + p.kblocks_per_split);
   const int nkb = kb1 - kb0;
@@ -510,12 +515,19 @@ __global__ void __launch_bounds__(kGramThreads, 1)
           break;
         }
         const uint32_t a = smem_u32(stage(s));
-        const int k = (kb0 + i) * BK;
+        const int gk = kb0 + i, seg = gk / kb_seg;
+        const int k = (gk - seg * kb_seg) * BK;
+        // segment 0: rows mt of A against rows nt of B; segment 1 swaps them
+        const bool one = p.nseg == 1;
+        const CUtensorMap* rh = seg ? &tmBH : &tmAH;
+        const CUtensorMap* rl = seg ? &tmBL : &tmAL;
+        const CUtensorMap* ch = (one || seg) ? &tmAH : &tmBH;
+        const CUtensorMap* cl = (one || seg) ? &tmAL : &tmBL;
         mbar_expect_tx(full0 + 8 * s, C::STAGE);
-        tma_load_3d(a, &tmH, k, mt * BM, z, full0 + 8 * s);
-        tma_load_3d(a + C::TILE, &tmL, k, mt * BM, z, full0 + 8 * s);
-        tma_load_3d(a + 2 * C::TILE, &tmH, k, nt * BN, z, full0 + 8 * s);
-        tma_load_3d(a + 3 * C::TILE, &tmL, k, nt * BN, z, full0 + 8 * s);
+        tma_load_3d(a, rh, k, mt * BM, z, full0 + 8 * s);
+        tma_load_3d(a + C::TILE, rl, k, mt * BM, z, full0 + 8 * s);
+        tma_load_3d(a + 2 * C::TILE, ch, k, nt * BN, z, full0 + 8 * s);
+        tma_load_3d(a + 3 * C::TILE, cl, k, nt * BN, z, full0 + 8 * s);
         *reinterpret_cast<volatile int*>(&ctrl->issued) = i + 1;
       }
     }
@@ -745,17 +757,18 @@ extern "C" int vqc_tc_half_transform(const float* b_aux_major, int32_t nmol, int
   return fail(VQC_STATUS_INVALID_ARGUMENT, "half_transform: o_pad");
 }
 
-extern "C" int vqc_tc_gram(const float* u_hi, const float* u_lo, int32_t nmol, int32_t nao,
-                           int32_t kdim, double* kout, int32_t* error, void* stream) {
-  if (!u_hi || !u_lo || !kout || nmol <= 0 || nao <= 0 || kdim <= 0 || kdim % 4)
-    return fail(VQC_STATUS_INVALID_ARGUMENT, "gram: bad argument");
-  CUtensorMap th, tl;
-  int st = make_map(&th, u_hi, kdim, kdim, nao, nmol, BM);
-  if (!st) st = make_map(&tl, u_lo, kdim, kdim, nao, nmol, BM);
+static int launch_gram(const float* a_hi, const float* a_lo, const float* b_hi, const float* b_lo,
+                       int nseg, int32_t nmol, int32_t nao, int32_t kdim, double* kout,
+                       int32_t* error, void* stream) {
+  CUtensorMap ah, al, bh, bl;
+  int st = make_map(&ah, a_hi, kdim, kdim, nao, nmol, BM);
+  if (!st) st = make_map(&al, a_lo, kdim, kdim, nao, nmol, BM);
+  if (!st) st = make_map(&bh, b_hi, kdim, kdim, nao, nmol, BM);
+  if (!st) st = make_map(&bl, b_lo, kdim, kdim, nao, nmol, BM);
   if (st) return st;
   const int nt = (nao + BM - 1) / BM;
   const int tiles = nt * (nt + 1) / 2;
-  const int kb_total = (kdim + BK - 1) / BK;
+  const int kb_total = (kdim + BK - 1) / BK * nseg;
   const int sms = sm_count();
   long long base = (long long)tiles * nmol;
   int ksplit = (int)((2LL * sms + base - 1) / base);
@@ -772,6 +785,7 @@ extern "C" int vqc_tc_gram(const float* u_hi, const float* u_lo, int32_t nmol, i
   p.ntiles_ut = tiles;
   p.kblocks_per_split = per;
   p.ksplit = ksplit;
+  p.nseg = nseg;
   p.kout = kout;
   p.error = error;
   static bool attr = false;
@@ -782,7 +796,22 @@ extern "C" int vqc_tc_gram(const float* u_hi, const float* u_lo, int32_t nmol, i
     attr = true;
   }
   dim3 grid(tiles, nmol * ksplit);
-  gram_ws_kernel<<<grid, kGramThreads, GramCfg::SMEM, (cudaStream_t)stream>>>(th, tl, p);
+  gram_ws_kernel<<<grid, kGramThreads, GramCfg::SMEM, (cudaStream_t)stream>>>(ah, al, bh, bl, p);
   count_launch();
   return cuda_status(cudaGetLastError(), "gram launch");
+}
+
+extern "C" int vqc_tc_gram(const float* u_hi, const float* u_lo, int32_t nmol, int32_t nao,
+                           int32_t kdim, double* kout, int32_t* error, void* stream) {
+  if (!u_hi || !u_lo || !kout || nmol <= 0 || nao <= 0 || kdim <= 0 || kdim % 4)
+    return fail(VQC_STATUS_INVALID_ARGUMENT, "gram: bad argument");
+  return launch_gram(u_hi, u_lo, u_hi, u_lo, 1, nmol, nao, kdim, kout, error, stream);
+}
+
+extern "C" int vqc_tc_gram_sym2(const float* a_hi, const float* a_lo, const float* b_hi,
+                                const float* b_lo, int32_t nmol, int32_t nao, int32_t kdim,
+                                double* kout, int32_t* error, void* stream) {
+  if (!a_hi || !a_lo || !b_hi || !b_lo || !kout || nmol <= 0 || nao <= 0 || kdim <= 0 || kdim % 4)
+    return fail(VQC_STATUS_INVALID_ARGUMENT, "gram_sym2: bad argument");
+  return launch_gram(a_hi, a_lo, b_hi, b_lo, 2, nmol, nao, kdim, kout, error, stream);
 }

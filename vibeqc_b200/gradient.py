@@ -27,10 +27,80 @@ from .jk import unpack_index
 from .timing import TIMER
 
 
-def _packed_rows(n: int, device) -> torch.Tensor:
-    """Row-major (mu >= nu) positions in the N*N square for every packed row."""
-    mu, nu = torch.tril_indices(n, n, device=device)
-    return mu * n + nu
+WEIGHT_ROW_BLOCK = 32  # AO rows per block of the packed Abar assembly
+SYM_BLOCK = 256  # row block of the triangular and symmetric products
+
+
+def _upper_times(w: torch.Tensor, g: torch.Tensor) -> torch.Tensor:
+    """W @ g for upper-triangular W (X, X): row block r needs rows >= r0 of g."""
+    x = w.shape[0]
+    out = torch.empty(x, g.shape[1], dtype=g.dtype, device=g.device)
+    for r0 in range(0, x, SYM_BLOCK):
+        r1 = min(x, r0 + SYM_BLOCK)
+        torch.mm(w[r0:r1, r0:], g[r0:], out=out[r0:r1])
+    return out
+
+
+def _sym_gram(g: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+    """g g^T from its upper block triangle (mirrored)."""
+    x = g.shape[0]
+    if out is None:
+        out = torch.empty(x, x, dtype=g.dtype, device=g.device)
+    for r0 in range(0, x, SYM_BLOCK):
+        r1 = min(x, r0 + SYM_BLOCK)
+        blk = g[r0:r1] @ g[r0:].T
+        out[r0:r1, r0:] = blk
+        out[r1:, r0:r1] = blk[:, r1 - r0:].T
+    return out
+
+
+_BLOCK_INDEX: dict = {}
+
+
+def _block_rows(n: int, m0: int, m1: int, device) -> torch.Tensor:
+    """Positions of the packed rows (mu in [m0, m1), nu <= mu) in a (m1-m0, m1) block."""
+    key = (n, m0, m1, str(device))
+    idx = _BLOCK_INDEX.get(key)
+    if idx is None:
+        mu = torch.arange(m0, m1, device=device)
+        nu = torch.arange(m1, device=device)
+        keep = nu[None, :] <= mu[:, None]
+        idx = ((mu[:, None] - m0) * m1 + nu[None, :])[keep]
+        _BLOCK_INDEX[key] = idx
+    return idx
+
+
+def molecule_weights(c: torch.Tensor, dens: torch.Tensor, rho: torch.Tensor, u: torch.Tensor,
+                     w: torch.Tensor, upper: bool, abar: torch.Tensor | None = None,
+                     mbar: torch.Tensor | None = None):
+    """Packed Abar (N(N+1)/2, X) and Mbar (X, X) of one molecule.
+
+    c (N, o) occupied factor (D = 2 c c^T), rho (X) whitened fitted density,
+    u (N, o, X) = B C (whitened), w (X, X) whitening factor (upper triangular
+    when ``upper``).  Abar rows are the packed pairs mu >= nu in row-major
+    order; each block of AO rows mu is one GEMM over nu < m1 followed by the
+    rank-one D (x) c term, so the full N*N*X tensor is never formed.
+    """
+    n, o, x = u.shape
+    cvec = w @ rho  # raw-basis fitting coefficients c = Minv rho
+    bij = torch.einsum("mi,mjq->qij", c, u).reshape(x, o * o)  # C^T B_Q C
+    gam = _upper_times(w, bij) if upper else w @ bij  # Gamma[P, ij]
+    del bij
+    # T[i][nu][P] = sum_j C[nu, j] Gamma[P, i, j]
+    t1 = torch.einsum("nj,pij->inp", c, gam.view(x, o, o)).reshape(o, n * x)
+    if abar is None:
+        abar = torch.empty(n * (n + 1) // 2, x, dtype=u.dtype, device=u.device)
+    mu_all, nu_all = torch.tril_indices(n, n, device=u.device)
+    dpairs = dens[mu_all, nu_all]
+    for m0 in range(0, n, WEIGHT_ROW_BLOCK):
+        m1 = min(n, m0 + WEIGHT_ROW_BLOCK)
+        blk = (c[m0:m1] @ t1[:, : m1 * x]).view(-1, x)  # (rows mu) x (nu < m1, P)
+        p0, p1 = m0 * (m0 + 1) // 2, m1 * (m1 + 1) // 2
+        torch.addr(blk[_block_rows(n, m0, m1, u.device)], dpairs[p0:p1], cvec, beta=-2.0,
+                   alpha=1.0, out=abar[p0:p1])
+    mbar = _sym_gram(gam, mbar)
+    mbar.addr_(cvec, cvec, alpha=-0.5)
+    return abar, mbar
 
 
 def df_rhf_gradient(chunk, ints, scf_out: dict, xyz: torch.Tensor) -> torch.Tensor:
@@ -54,23 +124,11 @@ def df_rhf_gradient(chunk, ints, scf_out: dict, xyz: torch.Tensor) -> torch.Tens
         rho_all, u_all = scf_out["exact_half"]  # FP64 U = B C already formed for the energy
     else:
         rho_all, u_all = jk.half_transform(c)  # fitted density and U = B C
-    rows = _packed_rows(n, dev)
-    abar = torch.empty(nb, rows.numel(), x, dtype=torch.float64, device=dev)
+    abar = torch.empty(nb, n * (n + 1) // 2, x, dtype=torch.float64, device=dev)
     mbar = torch.empty(nb, x, x, dtype=torch.float64, device=dev)
+    tri = mf.kind == "cholesky"
     for m in range(nb):  # per molecule: bounded temporaries
-        cvec = mf.inv_sqrt[m] @ rho_all[m]  # raw-basis c = Minv rho
-        u = u_all[m].to(torch.float64)  # (N(mu), X, o(j))
-        bij = torch.einsum("mi,mqj->qij", c[m], u)  # (X, o, o)
-        del u
-        gam = (mf.inv_sqrt[m] @ bij.reshape(x, o * o)).view(x, o, o)
-        t1 = torch.einsum("nj,pij->inp", c[m], gam).reshape(o, n * x)  # (o, N*X)
-        sq = (c[m] @ t1).view(n * n, x)  # (N*N, X) = sum_i C[mu i] T[i, nu, P]
-        del t1
-        sq = dens[m].reshape(n * n, 1) * cvec[None, :] - 2.0 * sq
-        abar[m] = sq[rows]
-        del sq
-        gflat = gam.reshape(x, o * o)
-        mbar[m] = -0.5 * torch.outer(cvec, cvec) + gflat @ gflat.T
+        molecule_weights(c[m], dens[m], rho_all[m], u_all[m], mf.inv_sqrt[m], tri, abar[m], mbar[m])
     wctx.__exit__(None, None, None)
     grad = torch.zeros(plan.natom * 3, dtype=torch.float64, device=dev)
     st = torch.cuda.current_stream().cuda_stream

@@ -9,8 +9,10 @@ as in ``src/scf/cuda/df_occupied_exchange.cpp:191-300``.
 transform U = B C and the Gram product K = 2 U U^T run on the tcgen05 tensor
 cores in split precision (3xTF32: round-to-nearest hi/lo parts, FP32
 accumulation drained to FP64); the fitted density rho = B^T d and J = B rho
-stream the FP32 B with FP64 accumulation.  The FP64 tensor stays resident for
-the finishing iterations, the final energy and the gradient.
+stream the FP32 B with FP64 accumulation.  Once the SCF is close to
+convergence the builds switch to increments about an FP64 anchor (see
+``MixedBuilder.anchor``), so the converged J, K, energy and the gradient
+operands carry FP64 accuracy.
 """
 
 from __future__ import annotations
@@ -45,11 +47,11 @@ class FP64Builder:
             rho = torch.bmm(d.reshape(nb, 1, n * n), b)  # (nb, 1, X)
             j = torch.bmm(b, rho.transpose(1, 2)).reshape(nb, n, n)
         with TIMER.stage("K_fp64"):
-            # U[b, mu, Q, i] = sum_nu B[mu, nu, Q] C[nu, i]
-            b4 = b.view(nb, n, n, x)
-            u = torch.matmul(b4.transpose(2, 3), c_occ[:, None, :, :])  # (nb, N, X, o)
-            u = u.reshape(nb, n, x * o)
-            k = 2.0 * torch.bmm(u, u.transpose(1, 2))
+            # U[i][mu][Q] = sum_nu C[nu, i] B[nu, mu Q] (B symmetric in mu, nu),
+            # K = 2 sum_i U_i U_i^T
+            ui = torch.bmm(c_occ.transpose(1, 2), b.view(nb, n, n * x)).view(nb * o, n, x)
+            k = 2.0 * torch.bmm(ui, ui.transpose(1, 2)).view(nb, o, n, n).sum(dim=1)
+            del ui
         self.nbuild += 1
         return j, k
 
@@ -59,14 +61,60 @@ class FP64Builder:
     def build_exact(self, d: torch.Tensor, c_occ: torch.Tensor):
         return self.build(d, c_occ)
 
-
     def half_transform(self, c_occ: torch.Tensor):
-        """(rho_whitened (nb, X), U (nb, N, X, o)) for D = 2 C C^T."""
-        nb, n, x, o = c_occ.shape[0], self.n, self.x, self.nocc
-        b4 = self.b.view(nb, n, n, x)
-        u = torch.matmul(b4.transpose(2, 3), c_occ[:, None, :, :])  # (nb, N, X, o)
-        rho = 2.0 * torch.einsum("bmi,bmqi->bq", c_occ, u)
-        return rho, u
+        """(rho_whitened (nb, X), U (nb, N, o, X)) for D = 2 C C^T."""
+        return fp64_half(self.b, c_occ, self.n, self.x)
+
+
+def fp64_half(b_full: torch.Tensor, c_occ: torch.Tensor, n: int, x: int):
+    """FP64 U[mu][i][Q] = sum_nu B[mu nu, Q] C[nu, i] and rho = 2 sum C U.
+
+    B is symmetric in (mu, nu), so B viewed as (nu, mu*Q) rows is one plain
+    GEMM per molecule, C^T (o x N) times (N x N*X); the result [i][mu][Q] is
+    permuted once to [mu][i][Q].
+    """
+    nb, o = c_occ.shape[0], c_occ.shape[2]
+    ui = torch.bmm(c_occ.transpose(1, 2), b_full.view(nb, n, n * x)).view(nb, o, n, x)
+    rho = 2.0 * torch.einsum("bmi,bimq->bq", c_occ, ui)
+    return rho, ui.transpose(1, 2).contiguous()
+
+
+HALF_BLOCK_BYTES = 1 << 28  # gathered FP64 rows per step of the packed half transform
+_GATHER: dict = {}
+
+
+def _gather_rows(n: int, m0: int, m1: int, device) -> torch.Tensor:
+    """Packed positions of the full rows (mu in [m0, m1), every nu)."""
+    key = (n, m0, m1, str(device))
+    idx = _GATHER.get(key)
+    if idx is None:
+        mu = torch.arange(m0, m1, device=device)[:, None]
+        nu = torch.arange(n, device=device)[None, :]
+        hi, lo = torch.maximum(mu, nu), torch.minimum(mu, nu)
+        idx = (hi * (hi + 1) // 2 + lo).reshape(-1)
+        _GATHER[key] = idx
+    return idx
+
+
+def fp64_half_packed(bp: torch.Tensor, c_occ: torch.Tensor, n: int, x: int):
+    """FP64 U[mu][i][Q] = sum_nu B[(mu nu), Q] C[nu, i] from packed rows, and rho.
+
+    Blocks of AO rows mu are gathered from the packed pairs into full rows
+    (bounded temporaries) and contracted with C by one batched GEMM per block,
+    written straight into the [mu][i][Q] layout.
+    """
+    nb, o = c_occ.shape[0], c_occ.shape[2]
+    u = torch.empty(nb, n, o, x, dtype=torch.float64, device=bp.device)
+    bm = max(1, min(n, HALF_BLOCK_BYTES // (8 * nb * n * x)))
+    ct = c_occ.transpose(1, 2)
+    for m0 in range(0, n, bm):
+        m1 = min(n, m0 + bm)
+        rows = torch.index_select(bp, 1, _gather_rows(n, m0, m1, bp.device))  # (nb, bm*N, X)
+        rows = rows.view(nb * (m1 - m0), n, x)
+        cexp = ct[:, None].expand(nb, m1 - m0, o, n).reshape(nb * (m1 - m0), o, n)
+        u[:, m0:m1] = torch.bmm(cexp, rows).view(nb, m1 - m0, o, x)
+    rho = 2.0 * torch.einsum("bmi,bmiq->bq", c_occ, u)
+    return rho, u
 
 
 def _round_up(v: int, m: int) -> int:
@@ -98,10 +146,8 @@ class MixedBuilder:
         self.u_hi = torch.zeros(nb, n, nocc, self.ldq, dtype=torch.float32, device=dev)
         self.u_lo = torch.zeros_like(self.u_hi)
         self.rho = torch.empty(nb, x, dtype=torch.float64, device=dev)
-        # the FP64 whitened tensor stays resident (full rows, as on the FP64
-        # path) for the FP64 finishing iterations, the final energy and the
-        # gradient weights
-        self.b64 = b_packed[:, unpack_index(n, dev), :].contiguous()  # (nb, N*N, X)
+        # the packed FP64 whitened tensor stays resident for the FP64 anchor
+        self.b64p = b_packed
         self.err = torch.zeros(1, dtype=torch.int32, device=dev)
         self.nbuild = 0
 
@@ -109,7 +155,9 @@ class MixedBuilder:
         if int(self.err.item()) != 0:
             raise self._lib.VqcError(6, f"tensor-core kernel wait expired (code {int(self.err.item())})")
 
-    def _half(self, c_occ: torch.Tensor):
+    def _half(self, c_occ: torch.Tensor, cvec: torch.Tensor | None = None,
+              rho: torch.Tensor | None = None):
+        """U = B c_occ into u_hi/u_lo; rho += 2 sum_{mu,i} U cvec (when given)."""
         nb, n, o = self.nb, self.n, self.nocc
         ct = torch.zeros(nb, o, self.ld, dtype=torch.float32, device=c_occ.device)
         ct[:, :, :n] = c_occ.transpose(1, 2)
@@ -117,12 +165,12 @@ class MixedBuilder:
         ct_lo = torch.empty_like(ct)
         self._lib.call("vqc_split_tf32", ct.data_ptr(), ct_hi.data_ptr(), ct_lo.data_ptr(),
                        ct.numel(), self.st)
-        c64 = c_occ.contiguous()
+        c64 = (c_occ if cvec is None else cvec).contiguous()
         with TIMER.stage("K_half_tc"):
             self._lib.call("vqc_tc_half_transform", self.b.data_ptr(), nb, n, self.ld, self.x,
                            ct_hi.data_ptr(), ct_lo.data_ptr(), c64.data_ptr(), o, self.o_pad,
-                           self.ldq, self.u_hi.data_ptr(), self.u_lo.data_ptr(), 0,
-                           self.err.data_ptr(), self.st)
+                           self.ldq, self.u_hi.data_ptr(), self.u_lo.data_ptr(),
+                           0 if rho is None else rho.data_ptr(), self.err.data_ptr(), self.st)
 
     def build(self, d: torch.Tensor, c_occ: torch.Tensor):
         nb, n = self.nb, self.n
@@ -144,39 +192,82 @@ class MixedBuilder:
         self._check()
         return j, 2.0 * k
 
-    def build_exact(self, d: torch.Tensor, c_occ: torch.Tensor):
-        """FP64 K and FP64-density J for the finishing iterations.
+    def half_transform(self, c_occ: torch.Tensor):
+        """FP64 (rho_whitened (nb, X), U (nb, N, o, X)) from the FP64 whitened tensor."""
+        with TIMER.stage("exact_half_fp64"):
+            return fp64_half_packed(self.b64p, c_occ, self.n, self.x)
 
-        K = 2 U U^T with U = B C in FP64 from the FP64 tensor; J streams the
-        FP32 B with the exact fitted density (the energy reported at the end is
-        re-evaluated fully in FP64, so the FP32 storage of B in J only shifts
-        the converged density at second order in the energy).
+    def release_tensor_core_buffers(self) -> None:
+        """Free the FP32 tensor and the split U/V buffers once the SCF is done."""
+        self.b = self.u_hi = self.u_lo = None
+        self.v_hi = self.v_lo = None
+
+    # -- incremental builds about an FP64 anchor ---------------------------
+    #
+    # J and K are linear in D.  At the anchor D0 = 2 C0 C0^T they are formed
+    # in FP64 (rho0, J0 = B rho0, U0 = B C0, K0 = 2 U0 U0^T).  Later
+    # iterations take C close to C0 (the occupied factor is aligned to C0),
+    # dC = C - C0, and only the increments run on the tensor cores:
+    #     dU = B dC,  rho = rho0 + 4 sum (C0 + dC/2) dU,  J = J0 + B (rho - rho0)
+    #     K = K0 + 2 (V dU^T + dU V^T),  V = U0 + dU / 2
+    # so their split-precision error scales with |D - D0| instead of |D|, and
+    # the converged operators are FP64-accurate.
+
+    def anchor(self, d: torch.Tensor, c_occ: torch.Tensor):
+        nb, n, x, o = self.nb, self.n, self.x, self.nocc
+        with TIMER.stage("anchor_fp64"):
+            rho0, u0 = fp64_half_packed(self.b64p, c_occ, n, x)  # u0 (nb, N, o, X)
+            uf = u0.view(nb, n, o * x)
+            k0 = 2.0 * torch.bmm(uf, uf.transpose(1, 2))
+            jp = torch.bmm(self.b64p, rho0[:, :, None])[:, :, 0]  # packed pairs
+            j0 = jp[:, unpack_index(n, d.device)].view(nb, n, n)
+        self.c0 = c_occ.clone()
+        self.rho0, self.j0, self.k0, self.u0 = rho0, j0, k0, u0
+        if not hasattr(self, "v_hi"):
+            self.v_hi = torch.empty_like(self.u_hi)
+            self.v_lo = torch.empty_like(self.u_hi)
+        self.nbuild += 1
+        return j0, k0, rho0
+
+    def _increment(self, c_occ: torch.Tensor):
+        """dU = B (C - C0) into u_hi/u_lo; returns rho - rho0."""
+        dc = c_occ - self.c0
+        drho = torch.zeros(self.nb, self.x, dtype=torch.float64, device=c_occ.device)
+        self._half(dc, cvec=self.c0 + 0.5 * dc, rho=drho)  # drho = 2 sum (C0 + dC/2) dU
+        return 2.0 * drho
+
+    def build_incremental(self, d: torch.Tensor, c_occ: torch.Tensor):
+        nb, n, x, o = self.nb, self.n, self.x, self.nocc
+        drho = self._increment(c_occ)
+        dj = torch.empty(nb, n, n, dtype=torch.float64, device=d.device)
+        with TIMER.stage("J_fp32"):
+            self._lib.call("vqc_coulomb_fp32", self.b.data_ptr(), drho.data_ptr(), nb, n,
+                           self.ld, x, dj.data_ptr(), self.st)
+        with TIMER.stage("K_gram_tc"):
+            self._lib.call("vqc_anchor_combine", self.u0.data_ptr(), self.u_hi.data_ptr(),
+                           self.u_lo.data_ptr(), self.v_hi.data_ptr(), self.v_lo.data_ptr(),
+                           nb * n * o, x, self.ldq, 0.5, 0, self.st)
+            kh = 0.5 * self.k0
+            self._lib.call("vqc_tc_gram_sym2", self.v_hi.data_ptr(), self.v_lo.data_ptr(),
+                           self.u_hi.data_ptr(), self.u_lo.data_ptr(), nb, n, o * self.ldq,
+                           kh.data_ptr(), self.err.data_ptr(), self.st)
+        self.nbuild += 1
+        self._check()
+        return self.j0 + dj, 2.0 * kh, self.rho0 + drho
+
+    def anchored_half(self, c_occ: torch.Tensor):
+        """(rho, U = U0 + B (C - C0)) at the final orbitals, FP64 (nb, N, o, X).
+
+        Consumes the anchor: U0 is updated in place.
         """
         nb, n, x, o = self.nb, self.n, self.x, self.nocc
-        rho, u = self.half_transform(c_occ)
-        j = torch.empty(nb, n, n, dtype=torch.float64, device=d.device)
-        with TIMER.stage("J_fp32"):
-            self._lib.call("vqc_coulomb_fp32", self.b.data_ptr(), rho.data_ptr(), nb, n,
-                           self.ld, x, j.data_ptr(), self.st)
-        with TIMER.stage("K_exact_fp64"):
-            uf = u.reshape(nb, n, x * o)
-            k = 2.0 * torch.bmm(uf, uf.transpose(1, 2))
-        self.nbuild += 1
-        return j, k
-
-    def half_transform(self, c_occ: torch.Tensor):
-        """FP64 (rho_whitened (nb, X), U (nb, N, X, o)) from the FP64 whitened tensor.
-
-        Used by the finishing iterations, the final energy and the gradient
-        weights, so the reported energy and forces carry no FP32 storage or
-        tensor-core error.
-        """
-        nb, n, x = self.nb, self.n, self.x
-        with TIMER.stage("exact_half_fp64"):
-            b4 = self.b64.view(nb, n, n, x)
-            u = torch.matmul(b4.transpose(2, 3), c_occ[:, None, :, :])  # (nb, N, X, o)
-            rho = 2.0 * torch.einsum("bmi,bmqi->bq", c_occ, u)
-        return rho, u
+        drho = self._increment(c_occ)
+        self._lib.call("vqc_anchor_combine", self.u0.data_ptr(), self.u_hi.data_ptr(),
+                       self.u_lo.data_ptr(), 0, 0, nb * n * o, x, self.ldq, 1.0, 1, self.st)
+        self._check()
+        u = self.u0
+        self.u0 = None
+        return self.rho0 + drho, u
 
 
 def make_builder(precision: str, b_packed: torch.Tensor, n: int, x: int, nocc: int):

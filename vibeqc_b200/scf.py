@@ -145,8 +145,9 @@ def factor_metric(metric: torch.Tensor, relative_threshold: float = 1e-10) -> Me
     return MetricFactor(lam, vec, keep, inv_sqrt, rank, cond, "eigen")
 
 
-MIXED_ITERATION_CAP = 40  # tensor-core iterations before the FP64 phase is forced
-TC_COMMUTATOR_EXIT = 1e-5  # max|FDS - SDF| that ends the tensor-core phase
+MIXED_ITERATION_CAP = 40  # plain tensor-core iterations before the anchor is forced
+ANCHOR_COMMUTATOR = 1e-5  # max|FDS - SDF| at which the FP64 anchor is formed
+ANCHOR_DIIS_RESET = False  # restart DIIS at the anchor
 
 
 def exact_energy(jk, d: torch.Tensor, c: torch.Tensor, h: torch.Tensor,
@@ -157,7 +158,7 @@ def exact_energy(jk, d: torch.Tensor, c: torch.Tensor, h: torch.Tensor,
     ej = 0.5 * (rho * rho).sum(dim=1)
     ek = torch.zeros_like(ej)
     for m in range(d.shape[0]):
-        bij = torch.einsum("mi,mqj->qij", c[m], u[m])
+        bij = torch.einsum("mi,mjq->qij", c[m], u[m])
         ek[m] = -(bij * bij).sum()
     return e1 + ej + ek + enuc, (rho, u)
 
@@ -191,16 +192,57 @@ def _orthogonalizer(s: torch.Tensor) -> torch.Tensor:
     return (vec * lam.rsqrt()[:, None, :]) @ vec.transpose(1, 2)
 
 
+SP2_GRAPH_STEPS = 8  # SP2 steps per captured CUDA graph (even: ends in the same buffer)
+# native kernels launched by graph replays (the library's own launch counter
+# sees only direct launches)
+GRAPH_LAUNCHES = [0]
+
+
+class _SP2Graph:
+    """SP2_GRAPH_STEPS SP2 steps (batched DGEMM + vqc_sp2_update) as one CUDA graph.
+
+    The iterate lives in static buffers; converged molecules are copied
+    unchanged by the update kernel, so extra steps are harmless and the host
+    reads the device flags once per replay.
+    """
+
+    def __init__(self, nb: int, n: int, nocc: int, tol: float, device):
+        self.x = torch.zeros(nb, n, n, dtype=torch.float64, device=device)
+        self.x2 = torch.empty_like(self.x)
+        self.xn = torch.empty_like(self.x)
+        self.done = torch.zeros(nb, dtype=torch.int32, device=device)
+        self.args = (nb, n, float(nocc), float(tol))
+        side = torch.cuda.Stream(device=device)
+        side.wait_stream(torch.cuda.current_stream(device))
+        with torch.cuda.stream(side):  # warm-up outside capture (cuBLAS handles, workspaces)
+            self._steps()
+        torch.cuda.current_stream(device).wait_stream(side)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self._steps()
+
+    def _steps(self):
+        nb, n, nocc, tol = self.args
+        st = torch.cuda.current_stream().cuda_stream
+        x, xn = self.x, self.xn
+        for _ in range(SP2_GRAPH_STEPS):
+            torch.bmm(x, x, out=self.x2)
+            _lib.call("vqc_sp2_update", x.data_ptr(), self.x2.data_ptr(), xn.data_ptr(), nb, n,
+                      nocc, tol, self.done.data_ptr(), st)
+            x, xn = xn, x
+
+
 def purify_sp2(fo: torch.Tensor, nocc: int, max_steps: int = 96, tol: float = 1e-11,
-               check_every: int = 8) -> torch.Tensor:
+               graphs: dict | None = None) -> torch.Tensor:
     """Projector onto the lowest ``nocc`` eigenvectors of symmetric ``fo``.
 
     Second-order spectral projection (Niklasson, Phys. Rev. B 66, 155115
     (2002)): map the spectrum into [0, 1] with Gershgorin bounds, then apply
     X <- X^2 or X <- 2X - X^2, whichever moves tr X toward ``nocc``, until
     tr(X) - tr(X^2) < tol.  Per step: one batched GEMM and one native update
-    kernel (vqc_sp2_update); convergence flags stay on the device and are read
-    every ``check_every`` steps.
+    kernel (vqc_sp2_update); convergence flags stay on the device.  Steps run
+    in CUDA graphs of SP2_GRAPH_STEPS (cached in ``graphs``, one per shape and
+    tolerance), and the flags are read once per graph replay.
     """
     nb, n, _ = fo.shape
     diag = torch.diagonal(fo, dim1=1, dim2=2)
@@ -208,31 +250,34 @@ def purify_sp2(fo: torch.Tensor, nocc: int, max_steps: int = 96, tol: float = 1e
     emin = (diag - radius).min(dim=1).values
     emax = (diag + radius).max(dim=1).values
     eye = torch.eye(n, dtype=fo.dtype, device=fo.device)
-    x = ((emax[:, None, None] * eye - fo) / (emax - emin)[:, None, None]).contiguous()
-    x2 = torch.empty_like(x)
-    xn = torch.empty_like(x)
-    done = torch.zeros(nb, dtype=torch.int32, device=fo.device)
-    st = torch.cuda.current_stream().cuda_stream
-    for step in range(max_steps):
-        torch.bmm(x, x, out=x2)
-        _lib.call("vqc_sp2_update", x.data_ptr(), x2.data_ptr(), xn.data_ptr(), nb, n,
-                  float(nocc), tol, done.data_ptr(), st)
-        x, xn = xn, x
-        if step % check_every == check_every - 1 and bool(done.all()):
+    key = (nb, n, int(nocc), float(tol))
+    if graphs is None:
+        graphs = {}
+    g = graphs.get(key)
+    if g is None:
+        g = graphs[key] = _SP2Graph(nb, n, nocc, tol, fo.device)
+    torch.div(emax[:, None, None] * eye - fo, (emax - emin)[:, None, None], out=g.x)
+    g.done.zero_()
+    for _ in range(0, max_steps, SP2_GRAPH_STEPS):
+        g.graph.replay()
+        GRAPH_LAUNCHES[0] += SP2_GRAPH_STEPS
+        if bool(g.done.all()):
             break
-    return 0.5 * (x + x.transpose(1, 2))
+    return 0.5 * (g.x + g.x.transpose(1, 2))
 
 
-def occupied_factor(proj: torch.Tensor, guess: torch.Tensor, gen: torch.Generator) -> torch.Tensor:
+def occupied_factor(proj: torch.Tensor, guess: torch.Tensor, gen: torch.Generator,
+                    noise_scale: float = 0.3) -> torch.Tensor:
     """Orthonormal basis of range(proj) by Cholesky-QR2 of proj @ (guess + noise).
 
     The previous occupied factor plus a random component keeps proj @ guess
     full rank even when the occupied space rotates far between iterations;
     a molecule whose factorisation still fails is retried with a purely random
-    start.
+    start.  With ``noise_scale=0`` the result is the projected guess made
+    orthonormal, so it stays within O(|proj - guess guess^T|) of ``guess``.
     """
     noise = torch.randn(guess.shape, dtype=guess.dtype, device=guess.device, generator=gen)
-    start = guess + 0.3 * noise
+    start = guess + noise_scale * noise
     for attempt in range(2):
         y = torch.bmm(proj, start)
         ok = torch.ones(y.shape[0], dtype=torch.bool, device=y.device)
@@ -247,6 +292,32 @@ def occupied_factor(proj: torch.Tensor, guess: torch.Tensor, gen: torch.Generato
             return y
         start = torch.where(ok[:, None, None], start, noise)
     raise FloatingPointError("occupied-space factorisation failed")
+
+
+WHITEN_COLUMN_BLOCK = 256
+
+
+def whiten_in_place(a: torch.Tensor, mf: MetricFactor) -> None:
+    """B = A W over the packed rows of every molecule, in place (FP64 GEMMs).
+
+    Row blocks of all molecules of the chunk go through batched GEMMs with
+    bounded temporaries.  The Cholesky factor W = L^-T is upper triangular, so
+    column block [c0, c1) of B needs only columns < c1 of A: blocks are formed
+    right to left (each reads columns that are still unwhitened), which skips
+    the structural zeros of W and halves the flops of the dense product.
+    """
+    nb, p_rows, x = a.shape
+    w = mf.inv_sqrt
+    blk = max(256, (1 << 28) // (8 * x * nb))  # ~256 MB of rows per step
+    cb = WHITEN_COLUMN_BLOCK
+    for r0 in range(0, p_rows, blk):
+        rows = a[:, r0:r0 + blk]
+        if mf.kind != "cholesky":
+            rows.copy_(torch.matmul(rows, w))
+            continue
+        for c0 in range(((x - 1) // cb) * cb, -1, -cb):
+            c1 = min(x, c0 + cb)
+            rows[:, :, c0:c1].copy_(torch.matmul(rows[:, :, :c1], w[:, :c1, c0:c1]))
 
 
 def _diis_extrapolate(errs: list, focks: list) -> torch.Tensor:
@@ -278,14 +349,9 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
     with TIMER.stage("metric_factor"):
         mf = factor_metric(ints.metric, relative_threshold)
     with TIMER.stage("whiten"):
-        b_packed = ints.a_packed  # whitened in place: B = A W, row blocks
+        b_packed = ints.a_packed  # whitened in place: B = A W
         ints.a_packed = None  # the raw tensor is not needed after whitening
-        p_rows = b_packed.shape[1]
-        blk = max(1024, (1 << 27) // (8 * x))  # ~128 MB temporaries
-        for m in range(nb):
-            for r0 in range(0, p_rows, blk):
-                rows = b_packed[m, r0:r0 + blk]
-                rows.copy_(rows @ mf.inv_sqrt[m])  # GEMM: measured faster than DTRSM here
+        whiten_in_place(b_packed, mf)
         jk = jkmod.make_builder(precision, b_packed, n, x, nocc)
         del b_packed
     s, h = ints.s, ints.h
@@ -306,10 +372,12 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
     gen.manual_seed(1234)
     guess = torch.randn(nb, n, nocc, dtype=torch.float64, device=dev, generator=gen)
 
-    def density_from(f, guess, tol=1e-11):
+    sp2_graphs: dict = {}
+
+    def density_from(f, guess, tol=1e-11, noise_scale=0.3):
         with TIMER.stage("purify"):
-            proj = purify_sp2(xo.transpose(1, 2) @ f @ xo, nocc, tol=tol)
-            co = occupied_factor(proj, guess, gen)  # orthonormal, orthogonal basis
+            proj = purify_sp2(xo.transpose(1, 2) @ f @ xo, nocc, tol=tol, graphs=sp2_graphs)
+            co = occupied_factor(proj, guess, gen, noise_scale)  # orthonormal, orthogonal basis
         return 2.0 * (xo @ proj @ xo.transpose(1, 2)), co
 
     d, co = density_from(h, guess)
@@ -327,18 +395,31 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
     errs, focks = [], []
     comm_tol = 10.0 * min(1e-8, density_tolerance)
     # mixed precision runs two phases per chunk:
-    #   "tc":    tensor-core J/K until max|FDS-SDF| <= TC_COMMUTATOR_EXIT for every
-    #            active molecule (or MIXED_ITERATION_CAP).  The commutator
-    #            converges normally on these operators; their energy jitters by
-    #            ~1e-5 Eh between iterations, so energy is not the exit test.
-    #   "exact": FP64 J/K from the FP64 whitened rows, DIIS restarted, under
-    #            the reference's criteria (typically two or three iterations).
+    #   "tc":     plain tensor-core J/K until max|FDS-SDF| <= ANCHOR_COMMUTATOR
+    #             for every active molecule (or MIXED_ITERATION_CAP).  Their
+    #             split-precision error (~1e-7 relative, varying with D) makes
+    #             the energy jitter, so no convergence test runs here.
+    #   "anchor": one FP64 J/K build at the current density, then tensor-core
+    #             increments about it (MixedBuilder.build_incremental) with the
+    #             occupied factor aligned to the anchor's; the operators are
+    #             FP64-accurate and the reference's criteria apply.
+    # the FP64 path runs "exact" FP64 builds throughout.
     phase = "tc" if jk.precision == "mixed" else "exact"
     mixed_iterations = 0
     phase_iterations = 0
+    co_anchor = None
+    anchored = False
     for it in range(1, max_iterations + 1):
+        rho = None
         if phase == "exact":
             j, k = jk.build_exact(d, c)
+        elif phase == "anchor":
+            if not anchored:
+                j, k, rho = jk.anchor(d, c)
+                anchored = True
+            else:
+                j, k, rho = jk.build_incremental(d, c)
+                mixed_iterations += 1
         else:
             j, k = jk.build(d, c)
             mixed_iterations += 1
@@ -346,7 +427,12 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
         TIMER_ctx = TIMER.stage("scf_other")
         TIMER_ctx.__enter__()
         f = h + j - 0.5 * k
-        energy = 0.5 * torch.einsum("bmn,bmn->b", d, h + f) + enuc
+        if rho is not None:
+            # E = tr(D H) + |rho|^2 / 2 - tr(D K) / 4 + E_nn from the FP64-accurate rho, K
+            energy = (torch.einsum("bmn,bmn->b", d, h) + 0.5 * (rho * rho).sum(dim=1)
+                      - 0.25 * torch.einsum("bmn,bmn->b", d, k) + enuc)
+        else:
+            energy = 0.5 * torch.einsum("bmn,bmn->b", d, h + f) + enuc
         fds = f @ d @ s
         comm = fds - fds.transpose(1, 2)
         err = xo.transpose(1, 2) @ comm @ xo
@@ -356,7 +442,12 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
         f_ext = _diis_extrapolate(errs, focks) if len(errs) > 1 else f
         TIMER_ctx.__exit__(None, None, None)
         # the tensor-core phase only needs the projector to its own accuracy
-        d_new, co = density_from(f_ext, co, 1e-11 if phase == "exact" else 1e-8)
+        if phase == "anchor":
+            if co_anchor is None:
+                co_anchor = co
+            d_new, co = density_from(f_ext, co_anchor, 1e-11, 0.0)
+        else:
+            d_new, co = density_from(f_ext, co, 1e-11 if phase == "exact" else 1e-8)
         TIMER_ctx = TIMER.stage("scf_other")
         TIMER_ctx.__enter__()
         c_new = xo @ co
@@ -366,10 +457,11 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
         cmax = comm.abs().amax(dim=(1, 2))
         done = (de < energy_tolerance) & (drms < density_tolerance) & (cmax <= comm_tol)
         if phase == "tc":
-            loose = cmax <= TC_COMMUTATOR_EXIT
+            loose = cmax <= ANCHOR_COMMUTATOR
             if bool((loose | ~active).all()) or phase_iterations >= MIXED_ITERATION_CAP:
-                phase, phase_iterations = "exact", 0
-                errs, focks = [], []  # restart DIIS on the FP64 operators
+                phase, phase_iterations = "anchor", 0
+                if ANCHOR_DIIS_RESET:
+                    errs, focks = [], []
             done = torch.zeros_like(done)
         if trace is not None:
             trace.append((it, phase, float(de[active].max()) if bool(active.any()) else 0.0,
@@ -393,11 +485,14 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
         d = torch.where(active[:, None, None], d_new, d)
         c = torch.where(active[:, None, None], c_new, c)
         TIMER_ctx.__exit__(None, None, None)
-    if jk.precision == "mixed":
-        # final energy in FP64 arithmetic at the converged density: the SCF
-        # operators above carry the tensor cores' accumulation error, the
-        # energy is variational in D, so re-evaluating E[D] removes it to
-        # second order (the FP32 storage of B remains)
+    if jk.precision == "mixed" and anchored:
+        # rho and U = B C at the converged orbitals for the gradient: the
+        # anchor's FP64 U0 plus the tensor-core increment
+        exact_half = jk.anchored_half(c_final)
+        jk.release_tensor_core_buffers()
+    elif jk.precision == "mixed":
+        # never anchored (iteration limit in the plain tensor-core phase):
+        # re-evaluate E[D] in FP64 at the last density
         final_e, exact_half = exact_energy(jk, d_final, c_final, h, enuc)
     else:
         exact_half = None
