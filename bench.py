@@ -38,15 +38,23 @@ BASIS, AUX = "def2-svp", "cc-pvdz-jkfit"
 CPU_SAMPLE_SIZES = (2, 3, 4)
 
 
+SIZES = (2, 16)  # n ~ U{2..16}; --cluster-size N fixes n (a single-chunk case for profiling)
+
+
 def workload(count: int, seed: int):
     from vibeqc_b200 import geometry
 
-    return geometry.water_cluster_batch(count, 2, 16, seed)
+    return geometry.water_cluster_batch(count, SIZES[0], SIZES[1], seed)
 
 
 def workload_sizes(count: int, seed: int) -> np.ndarray:
     rng = np.random.default_rng(seed)
-    return rng.integers(2, 17, size=count)
+    return rng.integers(SIZES[0], SIZES[1] + 1, size=count)
+
+
+def workload_name(count: int) -> str:
+    dist = f"n~U{{{SIZES[0]}..{SIZES[1]}}}" if SIZES[0] != SIZES[1] else f"n={SIZES[0]}"
+    return f"{count} (H2O)n clusters, {dist}, def2-SVP/cc-pVDZ-JKFIT, energy+forces"
 
 
 def cpu_reference_step(count: int, seed: int) -> dict:
@@ -265,8 +273,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else "tf32x3/f32/f64",
         "data": "synthetic",
-        "config": {"workload": f"{args.count} (H2O)n clusters, n~U{{2..16}}, def2-SVP/cc-pVDZ-JKFIT, "
-                               "energy+forces", "precision": args.precision, "molecules_per_gpu": args.count,
+        "config": {"workload": workload_name(args.count), "precision": args.precision, "molecules_per_gpu": args.count,
                    "l2": "working set (B tensor, GBs) exceeds L2; no flush needed"},
         "e2e": {"value": round(e2e_value, 3), "unit": "mol/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
@@ -275,6 +282,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         "clocks": clocks.summary(),
         "roofline": rl,
         "stages_ms_per_step": {k: round(v["ms"] / steps, 3) for k, v in stages.items()},
+        "allocator": {"alloc_retries": int(torch.cuda.memory_stats().get("num_alloc_retries", 0)),
+                      "peak_reserved_gb": round(torch.cuda.max_memory_reserved() / 2**30, 2)},
     }
     if compare is not None:
         out["mixed_vs_fp64"] = compare
@@ -312,7 +321,14 @@ def main() -> int:
     ap.add_argument("--count", type=int, default=256)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cluster-size", type=int, default=0,
+                    help="every molecule (H2O)_n with this n (one homogeneous chunk, for profiling)")
     args = ap.parse_args()
+    global SIZES
+    if args.cluster_size:
+        if not 1 <= args.cluster_size <= 64:
+            ap.error("--cluster-size must be in 1..64")
+        SIZES = (args.cluster_size, args.cluster_size)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
@@ -334,8 +350,7 @@ def main() -> int:
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(wall / args.steps * 1000, 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": f"{args.count} (H2O)n clusters, n~U{{2..16}}, def2-SVP/cc-pVDZ-JKFIT, "
-                                   "energy+forces", "precision": "fp64"},
+            "config": {"workload": workload_name(args.count), "precision": "fp64"},
             "cpu_baseline": {"value": round(v, 6), "unit": "mol/s", "cores": cores, "kind": "port",
                              "sample": f"oracle DF-RHF E+F on (H2O)n n={list(CPU_SAMPLE_SIZES)}, "
                                        f"power-law fit (exponent {vals[-1]['fit_exponent']:.2f}) "

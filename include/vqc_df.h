@@ -159,8 +159,9 @@ int vqc_sp2_update(const double* x, const double* x2, double* xout, int32_t nmol
  *   vqc_coulomb_fp32: J[mol][mu][nu] = sum_Q B[mu][Q][nu] rho[mol][Q] (FP64
  *     accumulate); reference src/scf/cuda/df_coulomb.cpp:24.
  *   vqc_fitted_density_fp32: rho[mol][Q] = sum_{mu,nu} B[mu][Q][nu] D[mu][nu]
- *     for symmetric D [mol][nao][nao] (FP64 accumulate); reference
- *     df_coulomb.cpp:38-57.
+ *     for symmetric D [mol][nao][nao] (FP64 accumulate, deterministic);
+ *     partial: caller-owned workspace of nmol * nao * naux doubles (the
+ *     per-AO-row partial sums); reference df_coulomb.cpp:38-57.
  *   vqc_anchor_combine: with the FP64 anchor u0[rows][x] and the split
  *     increment du_hi/du_lo[rows][ld_aux]: mode 0 writes the split
  *     V = u0 + alpha (du_hi + du_lo) into v_hi/v_lo[rows][ld_aux] (padding
@@ -188,7 +189,8 @@ int vqc_anchor_combine(double* u0, const float* du_hi, const float* du_lo, float
 int vqc_coulomb_fp32(const float* b_aux_major, const double* rho, int32_t nmol, int32_t nao,
                      int32_t ld_ao, int32_t naux, double* j, void* stream);
 int vqc_fitted_density_fp32(const float* b_aux_major, const double* dens, int32_t nmol,
-                            int32_t nao, int32_t ld_ao, int32_t naux, double* rho, void* stream);
+                            int32_t nao, int32_t ld_ao, int32_t naux, double* partial, double* rho,
+                            void* stream);
 
 #ifdef __cplusplus
 }

@@ -101,7 +101,7 @@ _SIGNATURES = {
     "vqc_anchor_combine": ([_P, _P, _P, _P, _P, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32,
                             ctypes.c_double, ctypes.c_int32, _P], ctypes.c_int),
     "vqc_fitted_density_fp32": ([_P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
-                                 ctypes.c_int32, _P, _P], ctypes.c_int),
+                                 ctypes.c_int32, _P, _P, _P], ctypes.c_int),
     "vqc_coulomb_fp32": ([_P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                           ctypes.c_int32, _P, _P], ctypes.c_int),
 }

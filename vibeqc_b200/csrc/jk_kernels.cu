@@ -67,51 +67,51 @@ __global__ void __launch_bounds__(kJThreads)
 }
 
 // Fitted density rho[mol][Q] = sum_{mu,nu} B[mu][Q][nu] D[mu][nu] (D symmetric),
-// read from the nu <= mu half with weights 2 (nu < mu) and 1 (nu = mu).  One
-// CTA per (molecule, 32-row Q block) walks every mu; each of its 8 warps owns
-// 4 Q rows and reads them float4-wise along nu, so rho accumulates in
-// registers (FP64) without atomics.  Reference: rho = B^T vec(D) of
-// src/scf/cuda/df_coulomb.cpp:38-57 (FP64 cublasDgemv).
-constexpr int kRhoRows = 32;
+// read from the nu <= mu half with weights 2 (nu < mu) and 1 (nu = mu).
+// Stage 1: one CTA per (molecule, mu), shaped like the Coulomb kernel (8
+// warps split the Q rows, lanes read float4 along nu against the weighted
+// density row staged in shared memory), writes the row partial
+// part[mol][mu][Q] (FP64, warp-shuffle sums).  Stage 2 adds the partials over
+// mu in a fixed order, so the result is deterministic.  Reference:
+// rho = B^T vec(D) of src/scf/cuda/df_coulomb.cpp:38-57 (FP64 cublasDgemv).
+__global__ void __launch_bounds__(kJThreads)
+    fitted_rows_fp32_kernel(const float* __restrict__ b, const double* __restrict__ d, int n,
+                            int x, int ld, double* __restrict__ part) {
+  extern __shared__ double sw[];  // weighted density row, ld entries
+  const int mol = blockIdx.y, mu = blockIdx.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const double* drow = d + ((size_t)mol * n + mu) * n;
+  for (int nu = threadIdx.x; nu < ld; nu += kJThreads)
+    sw[nu] = nu < mu ? 2.0 * drow[nu] : (nu == mu ? drow[nu] : 0.0);
+  __syncthreads();
+  const float* rowb = b + ((size_t)mol * n + mu) * (size_t)x * ld;
+  const int nvec = (mu + 1 + 3) / 4;
+  double* out = part + ((size_t)mol * n + mu) * x;
+  for (int q = warp; q < x; q += kJWarps) {
+    const float4* p4 = reinterpret_cast<const float4*>(rowb + (size_t)q * ld);
+    double acc = 0.0;
+    for (int v = lane; v < nvec; v += 32) {
+      const float4 f = __ldg(p4 + v);
+      const double* w = sw + 4 * v;
+      acc = fma((double)f.x, w[0], acc);
+      acc = fma((double)f.y, w[1], acc);
+      acc = fma((double)f.z, w[2], acc);
+      acc = fma((double)f.w, w[3], acc);
+    }
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    if (lane == 0) out[q] = acc;
+  }
+}
 
 __global__ void __launch_bounds__(256)
-    fitted_density_fp32_kernel(const float* __restrict__ b, const double* __restrict__ d, int n,
-                               int x, int ld, double* __restrict__ rho) {
-  const int mol = blockIdx.y, q0 = blockIdx.x * kRhoRows;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const double* dm = d + (size_t)mol * n * n;
-  double acc[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int mu = 0; mu < n; ++mu) {
-    const int nvec = (mu + 1 + 3) / 4;
-    const double* drow = dm + (size_t)mu * n;
-    const float* bmu = b + ((size_t)mol * n + mu) * (size_t)x * ld;
-    for (int v = lane; v < nvec; v += 32) {
-      double w[4];
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int nu = 4 * v + e;
-        w[e] = nu < mu ? 2.0 * __ldg(drow + nu) : (nu == mu ? __ldg(drow + nu) : 0.0);
-      }
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const int q = q0 + warp * 4 + r;
-        if (q < x) {
-          const float4 f = __ldg(reinterpret_cast<const float4*>(bmu + (size_t)q * ld) + v);
-          acc[r] = fma((double)f.x, w[0], acc[r]);
-          acc[r] = fma((double)f.y, w[1], acc[r]);
-          acc[r] = fma((double)f.z, w[2], acc[r]);
-          acc[r] = fma((double)f.w, w[3], acc[r]);
-        }
-      }
-    }
-  }
-#pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    double s = acc[r];
-    for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
-    const int q = q0 + warp * 4 + r;
-    if (lane == 0 && q < x) rho[(size_t)mol * x + q] = s;
-  }
+    fitted_sum_kernel(const double* __restrict__ part, int n, int x, double* __restrict__ rho) {
+  const int mol = blockIdx.y;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= x) return;
+  const double* p = part + (size_t)mol * n * x + q;
+  double s = 0.0;
+  for (int mu = 0; mu < n; ++mu) s += p[(size_t)mu * x];
+  rho[(size_t)mol * x + q] = s;
 }
 
 // B[mol][mu][Q][nu] (FP32, ld) from the whitened packed rows
@@ -214,16 +214,23 @@ extern "C" int vqc_coulomb_fp32(const float* b_aux_major, const double* rho, int
 }
 
 extern "C" int vqc_fitted_density_fp32(const float* b_aux_major, const double* dens, int32_t nmol,
-                                       int32_t nao, int32_t ld_ao, int32_t naux, double* rho,
-                                       void* stream) {
-  if (!b_aux_major || !dens || !rho || nmol <= 0 || nao <= 0 || naux <= 0 || ld_ao < nao ||
-      ld_ao % 4 || nmol > 65535)
+                                       int32_t nao, int32_t ld_ao, int32_t naux, double* partial,
+                                       double* rho, void* stream) {
+  if (!b_aux_major || !dens || !partial || !rho || nmol <= 0 || nao <= 0 || naux <= 0 ||
+      ld_ao < nao || ld_ao % 4 || nmol > 65535 || nao > 0x7fffffff / 2)
     return fail(VQC_STATUS_INVALID_ARGUMENT, "fitted_density_fp32: bad argument");
-  dim3 grid((naux + kRhoRows - 1) / kRhoRows, nmol);
-  fitted_density_fp32_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(b_aux_major, dens, nao, naux,
-                                                                     ld_ao, rho);
+  const size_t smem = (size_t)ld_ao * sizeof(double);
+  if (smem > 48 * 1024) return fail(VQC_STATUS_INVALID_ARGUMENT, "fitted_density_fp32: nao too large");
+  dim3 g1(nao, nmol);
+  fitted_rows_fp32_kernel<<<g1, kJThreads, smem, (cudaStream_t)stream>>>(b_aux_major, dens, nao,
+                                                                         naux, ld_ao, partial);
   count_launch();
-  return cuda_status(cudaGetLastError(), "fitted_density_fp32");
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_status(e, "fitted_density_fp32 rows");
+  dim3 g2((naux + 255) / 256, nmol);
+  fitted_sum_kernel<<<g2, 256, 0, (cudaStream_t)stream>>>(partial, nao, naux, rho);
+  count_launch();
+  return cuda_status(cudaGetLastError(), "fitted_density_fp32 sum");
 }
 
 extern "C" int vqc_unpack_aux_major(const double* b_packed, int32_t nmol, int32_t nao, int32_t naux,

@@ -146,6 +146,7 @@ class MixedBuilder:
         self.u_hi = torch.zeros(nb, n, nocc, self.ldq, dtype=torch.float32, device=dev)
         self.u_lo = torch.zeros_like(self.u_hi)
         self.rho = torch.empty(nb, x, dtype=torch.float64, device=dev)
+        self.rho_part = torch.empty(nb, n, x, dtype=torch.float64, device=dev)
         # the packed FP64 whitened tensor stays resident for the FP64 anchor
         self.b64p = b_packed
         self.err = torch.zeros(1, dtype=torch.int32, device=dev)
@@ -181,7 +182,7 @@ class MixedBuilder:
             # tensor-core accumulation error in J), then J = B rho
             dd = d.contiguous()
             self._lib.call("vqc_fitted_density_fp32", self.b.data_ptr(), dd.data_ptr(), nb, n,
-                           self.ld, self.x, self.rho.data_ptr(), self.st)
+                           self.ld, self.x, self.rho_part.data_ptr(), self.rho.data_ptr(), self.st)
             self._lib.call("vqc_coulomb_fp32", self.b.data_ptr(), self.rho.data_ptr(), nb, n,
                            self.ld, self.x, j.data_ptr(), self.st)
         k = torch.zeros(nb, n, n, dtype=torch.float64, device=d.device)
@@ -201,6 +202,7 @@ class MixedBuilder:
         """Free the FP32 tensor and the split U/V buffers once the SCF is done."""
         self.b = self.u_hi = self.u_lo = None
         self.v_hi = self.v_lo = None
+        self.rho_part = None
 
     # -- incremental builds about an FP64 anchor ---------------------------
     #
@@ -253,7 +255,9 @@ class MixedBuilder:
                            kh.data_ptr(), self.err.data_ptr(), self.st)
         self.nbuild += 1
         self._check()
-        return self.j0 + dj, 2.0 * kh, self.rho0 + drho
+        # K = K0 + 2 (V dU^T + dU V^T) = K0 + (kh - K0/2) + (kh - K0/2)^T: the
+        # diagonal tiles' FP32 accumulation order leaves a tiny asymmetry
+        return self.j0 + dj, kh + kh.transpose(1, 2), self.rho0 + drho
 
     def anchored_half(self, c_occ: torch.Tensor):
         """(rho, U = U0 + B (C - C0)) at the final orbitals, FP64 (nb, N, o, X).

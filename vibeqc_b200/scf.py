@@ -232,6 +232,12 @@ class _SP2Graph:
             x, xn = xn, x
 
 
+# captured SP2 graphs by (chunk shape, n_occ, tolerance, device); kept for the
+# process so repeated executions of a prepared batch replay them
+_SP2_GRAPHS: dict = {}
+SP2_GRAPH_CACHE_BYTES = 4 << 30  # drop the cache when its buffers would exceed this
+
+
 def purify_sp2(fo: torch.Tensor, nocc: int, max_steps: int = 96, tol: float = 1e-11,
                graphs: dict | None = None) -> torch.Tensor:
     """Projector onto the lowest ``nocc`` eigenvectors of symmetric ``fo``.
@@ -250,11 +256,14 @@ def purify_sp2(fo: torch.Tensor, nocc: int, max_steps: int = 96, tol: float = 1e
     emin = (diag - radius).min(dim=1).values
     emax = (diag + radius).max(dim=1).values
     eye = torch.eye(n, dtype=fo.dtype, device=fo.device)
-    key = (nb, n, int(nocc), float(tol))
+    key = (nb, n, int(nocc), float(tol), str(fo.device))
     if graphs is None:
         graphs = {}
     g = graphs.get(key)
     if g is None:
+        held = sum(3 * v.x.numel() * 8 for v in graphs.values())
+        if held + 3 * nb * n * n * 8 > SP2_GRAPH_CACHE_BYTES:
+            graphs.clear()
         g = graphs[key] = _SP2Graph(nb, n, nocc, tol, fo.device)
     torch.div(emax[:, None, None] * eye - fo, (emax - emin)[:, None, None], out=g.x)
     g.done.zero_()
@@ -372,7 +381,7 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
     gen.manual_seed(1234)
     guess = torch.randn(nb, n, nocc, dtype=torch.float64, device=dev, generator=gen)
 
-    sp2_graphs: dict = {}
+    sp2_graphs = _SP2_GRAPHS
 
     def density_from(f, guess, tol=1e-11, noise_scale=0.3):
         with TIMER.stage("purify"):
