@@ -183,6 +183,18 @@ int vqc_tc_gram(const float* u_hi, const float* u_lo, int32_t nmol, int32_t nao,
 int vqc_tc_gram_sym2(const float* a_hi, const float* a_lo, const float* b_hi, const float* b_lo,
                      int32_t nmol, int32_t nao, int32_t kdim, double* kout, int32_t* error,
                      void* stream);
+/*
+ * vqc_fitted_density_fp32_noalloc: vqc_fitted_density_fp32 without the
+ * caller's workspace; the partial sums use a fixed device array of 4194304
+ * doubles (32 MiB) inside the library, so nmol * nao * naux must not exceed
+ * 4194304 (larger requests fail with VQC_STATUS_INVALID_ARGUMENT).  Allocates
+ * nothing; no buffer needs zeroing.  Calls that overlap on the GPU share the
+ * array and race: serialise them (one stream per device).  No counterpart in
+ * the reference.
+ */
+int vqc_fitted_density_fp32_noalloc(const float* b_aux_major, const double* dens, int32_t nmol,
+                                    int32_t nao, int32_t ld_ao, int32_t naux, double* rho,
+                                    void* stream);
 int vqc_anchor_combine(double* u0, const float* du_hi, const float* du_lo, float* v_hi,
                        float* v_lo, int64_t rows, int32_t x, int32_t ld_aux, double alpha,
                        int32_t mode, void* stream);

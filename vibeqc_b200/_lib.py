@@ -98,6 +98,8 @@ _SIGNATURES = {
                     ctypes.c_int),
     "vqc_tc_gram_sym2": ([_P, _P, _P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _P,
                           _P, _P], ctypes.c_int),
+    "vqc_fitted_density_fp32_noalloc": ([_P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                         ctypes.c_int32, _P, _P], ctypes.c_int),
     "vqc_anchor_combine": ([_P, _P, _P, _P, _P, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32,
                             ctypes.c_double, ctypes.c_int32, _P], ctypes.c_int),
     "vqc_fitted_density_fp32": ([_P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,

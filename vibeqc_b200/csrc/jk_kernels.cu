@@ -6,6 +6,8 @@
 // B[mu] (J is symmetric); its 8 warps split the Q range, lanes read float4
 // along nu, accumulate in FP64 with rho staged in shared memory, and the warp
 // partials are summed through shared memory into J[mu][nu] and J[nu][mu].
+#include <mutex>
+
 #include "vqc_df.h"
 #include "vqc_plan.hpp"
 
@@ -231,6 +233,54 @@ extern "C" int vqc_fitted_density_fp32(const float* b_aux_major, const double* d
   fitted_sum_kernel<<<g2, 256, 0, (cudaStream_t)stream>>>(partial, nao, naux, rho);
   count_launch();
   return cuda_status(cudaGetLastError(), "fitted_density_fp32 sum");
+}
+
+// No-allocation variant of vqc_fitted_density_fp32: the per-row partial sums
+// live in a file-scope device array of fixed capacity instead of a
+// caller-owned buffer.  Its address is taken once per device (with that
+// device current) by cudaGetSymbolAddress; nothing is allocated per call.
+// Nothing in the array must start at zero: stage 1 writes every partial the
+// launch's stage 2 reads.  Calls that overlap on the GPU (other streams,
+// devices sharing a context aside) share the array and race.
+constexpr size_t kFittedScratchDoubles = (size_t)1 << 22;  // 32 MiB
+static __device__ __align__(256) double g_fitted_scratch[kFittedScratchDoubles];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mutex;
+double* g_scratch_ptr[kMaxDevices] = {};
+}  // namespace
+
+static int fitted_scratch(double** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_status(e, "fitted_density_fp32_noalloc: device");
+  if (dev < 0 || dev >= kMaxDevices)
+    return fail(VQC_STATUS_INVALID_ARGUMENT, "fitted_density_fp32_noalloc: device index out of range");
+  std::lock_guard<std::mutex> lock(g_scratch_mutex);
+  if (!g_scratch_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_fitted_scratch);
+    if (e != cudaSuccess) return cuda_status(e, "fitted_density_fp32_noalloc: scratch address");
+    g_scratch_ptr[dev] = static_cast<double*>(p);
+  }
+  *out = g_scratch_ptr[dev];
+  return VQC_STATUS_SUCCESS;
+}
+
+extern "C" int vqc_fitted_density_fp32_noalloc(const float* b_aux_major, const double* dens,
+                                               int32_t nmol, int32_t nao, int32_t ld_ao,
+                                               int32_t naux, double* rho, void* stream) {
+  if (!b_aux_major || !dens || !rho || nmol <= 0 || nao <= 0 || naux <= 0)
+    return fail(VQC_STATUS_INVALID_ARGUMENT, "fitted_density_fp32_noalloc: bad argument");
+  const size_t need = (size_t)nmol * (size_t)nao * (size_t)naux;
+  if (need > kFittedScratchDoubles)
+    return fail(VQC_STATUS_INVALID_ARGUMENT,
+                "fitted_density_fp32_noalloc: nmol * nao * naux exceeds the 4194304-double scratch");
+  double* part = nullptr;
+  const int st = fitted_scratch(&part);
+  if (st) return st;
+  return vqc_fitted_density_fp32(b_aux_major, dens, nmol, nao, ld_ao, naux, part, rho, stream);
 }
 
 extern "C" int vqc_unpack_aux_major(const double* b_packed, int32_t nmol, int32_t nao, int32_t naux,
