@@ -184,13 +184,17 @@ int vqc_tc_gram_sym2(const float* a_hi, const float* a_lo, const float* b_hi, co
                      int32_t nmol, int32_t nao, int32_t kdim, double* kout, int32_t* error,
                      void* stream);
 /*
- * vqc_fitted_density_fp32_noalloc: vqc_fitted_density_fp32 without the
- * caller's workspace; the partial sums use a fixed device array of 4194304
- * doubles (32 MiB) inside the library, so nmol * nao * naux must not exceed
- * 4194304 (larger requests fail with VQC_STATUS_INVALID_ARGUMENT).  Allocates
- * nothing; no buffer needs zeroing.  Calls that overlap on the GPU share the
- * array and race: serialise them (one stream per device).  No counterpart in
- * the reference.
+ * vqc_fitted_density_fp32_noalloc: vqc_fitted_density_fp32 for callers that
+ * cannot allocate device memory (their GPU memory belongs to another
+ * allocator's pool, or they must avoid the synchronisation cudaFree implies).
+ * The caller passes only inputs and the output; the partial sums use a fixed
+ * device array of 4194304 doubles (32 MiB) inside the library, held on every
+ * GPU that loads it until exit, so nmol * nao * naux must not exceed 4194304
+ * (larger requests fail with VQC_STATUS_INVALID_ARGUMENT).  Allocates nothing.
+ * The first call on a device looks up the array's address (make it before
+ * any stream capture).  The array keeps the last call's contents and nothing
+ * in it needs zeroing.  Calls that overlap on the GPU share the array and
+ * race: serialise them.  No counterpart in the reference.
  */
 int vqc_fitted_density_fp32_noalloc(const float* b_aux_major, const double* dens, int32_t nmol,
                                     int32_t nao, int32_t ld_ao, int32_t naux, double* rho,

@@ -1,7 +1,12 @@
 """The no-allocation fitted-density entry point against the workspace one.
 
-Collected last (file name), so it runs both alone in a fresh process and after
-every other GPU test.
+The entry point serves callers that cannot allocate device memory (their GPU
+memory is owned by another allocator's pool, or they must avoid the
+synchronisation cudaFree implies): its partial sums live in a fixed array
+inside the library.  Two calls in a row must both reproduce the workspace
+entry point, so nothing left in the shared array from a previous call leaks
+into a result.  The file name makes pytest collect it last, so it runs alone in
+a fresh process and after every other GPU test.
 """
 
 import pytest

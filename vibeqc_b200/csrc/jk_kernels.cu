@@ -235,13 +235,18 @@ extern "C" int vqc_fitted_density_fp32(const float* b_aux_major, const double* d
   return cuda_status(cudaGetLastError(), "fitted_density_fp32 sum");
 }
 
-// No-allocation variant of vqc_fitted_density_fp32: the per-row partial sums
-// live in a file-scope device array of fixed capacity instead of a
-// caller-owned buffer.  Its address is taken once per device (with that
-// device current) by cudaGetSymbolAddress; nothing is allocated per call.
-// Nothing in the array must start at zero: stage 1 writes every partial the
-// launch's stage 2 reads.  Calls that overlap on the GPU (other streams,
-// devices sharing a context aside) share the array and race.
+// No-allocation variant of vqc_fitted_density_fp32, for callers that cannot
+// allocate device memory: a host program whose GPU memory is already owned by
+// another allocator's pool (a framework's caching allocator, a fixed arena),
+// or one that must not pay the device-wide synchronisation cudaFree implies.
+// The per-row partial sums live in a file-scope device array of fixed
+// capacity instead of a caller-owned buffer; every GPU that loads the library
+// holds it until the process exits.  The first call on a device takes the
+// array's device address with cudaGetSymbolAddress (that device current) and
+// caches it, so that first call should come before any stream capture.
+// Every call shares the array, which keeps the last call's contents; nothing
+// in it must start at zero, because stage 1 writes every partial that the
+// same launch's stage 2 reads.  Calls that overlap on the GPU race.
 constexpr size_t kFittedScratchDoubles = (size_t)1 << 22;  // 32 MiB
 static __device__ __align__(256) double g_fitted_scratch[kFittedScratchDoubles];
 
