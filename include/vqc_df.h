@@ -137,7 +137,8 @@ int vqc_sp2_update(const double* x, const double* x2, double* xout, int32_t nmol
 
 /*
  * Mixed-precision J/K over the FP32 whitened tensor stored aux-major per AO
- * row: b_aux_major[mol][mu][Q][nu], row length ld_ao >= nao (ld_ao % 4 == 0,
+ * row: b_aux_major[mol][mu][Q][nu], row length ld_ao >= nao (ld_ao % 4 == 0;
+ * the Coulomb and fitted-density kernels take ld_ao <= 512,
  * padding zero).  Replaces the FP64 packed/dense B of the reference's CUDA
  * plan (src/scf/cuda/df_plan_setup.cpp:70,224).
  *   vqc_unpack_aux_major: packed whitened FP64 rows -> b_aux_major (FP32).

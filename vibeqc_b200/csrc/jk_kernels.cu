@@ -3,9 +3,12 @@
 // Reference: src/scf/cuda/df_coulomb.cpp:24 (packed cublasDgemv, FP64).
 //
 // HBM-streaming: one CTA per (molecule, mu) reads only the nu <= mu half of
-// B[mu] (J is symmetric); its 8 warps split the Q range, lanes read float4
-// along nu, accumulate in FP64 with rho staged in shared memory, and the warp
-// partials are summed through shared memory into J[mu][nu] and J[nu][mu].
+// B[mu] (J is symmetric).  A row holds nvec = ceil((mu + 1) / 4) float4; each
+// warp splits into groups of L = min(32, pow2 >= nvec) lanes so short rows do
+// not idle lanes, and every group streams kJRows independent Q rows per pass
+// (memory-level parallelism).  Accumulation is FP64 with rho staged in shared
+// memory; group and warp partials are summed through shuffles and shared
+// memory into J[mu][nu] and J[nu][mu].
 #include <mutex>
 
 #include "vqc_df.h"
@@ -16,6 +19,13 @@ namespace vqc {
 constexpr int kJThreads = 256;          // 8 warps share the Q range of one (mol, mu) row
 constexpr int kJWarps = kJThreads / 32;
 constexpr int kJMaxVec = 4;             // float4 per lane: nu < 4 * 32 * 4 = 512
+constexpr int kJRows = 4;               // Q rows per lane group per pass
+
+__device__ __forceinline__ int group_lanes(int nvec) {
+  int l = 1;
+  while (l < nvec && l < 32) l <<= 1;
+  return l;
+}
 
 __global__ void __launch_bounds__(kJThreads)
     coulomb_fp32_kernel(const float* __restrict__ b, const double* __restrict__ rho, int n, int x,
@@ -29,32 +39,53 @@ __global__ void __launch_bounds__(kJThreads)
   __syncthreads();
   const float* rowb = b + ((size_t)mol * n + mu) * (size_t)x * ld;
   const int nvec = (mu + 1 + 3) / 4;  // float4 columns covering nu <= mu (ld % 4 == 0)
+  const int L = group_lanes(nvec), G = 32 / L, grp = lane / L, gl = lane % L;
+  const int rstride = kJWarps * G;  // lane groups per CTA
   double acc[kJMaxVec][4];
 #pragma unroll
   for (int t = 0; t < kJMaxVec; ++t)
 #pragma unroll
     for (int e = 0; e < 4; ++e) acc[t][e] = 0.0;
-  for (int q = warp; q < x; q += kJWarps) {
-    const double r = srho[q];
-    const float4* p4 = reinterpret_cast<const float4*>(rowb + (size_t)q * ld);
+  // q0 - grp is the same for every lane of the warp: the trip count is uniform
+  for (int q0 = warp * G + grp; q0 - grp < x; q0 += kJRows * rstride) {
 #pragma unroll
     for (int t = 0; t < kJMaxVec; ++t) {
-      const int v = lane + 32 * t;
+      const int v = gl + L * t;
       if (v < nvec) {
-        const float4 f = __ldg(p4 + v);
-        acc[t][0] = fma((double)f.x, r, acc[t][0]);
-        acc[t][1] = fma((double)f.y, r, acc[t][1]);
-        acc[t][2] = fma((double)f.z, r, acc[t][2]);
-        acc[t][3] = fma((double)f.w, r, acc[t][3]);
+        float4 f[kJRows];
+        double r[kJRows];
+#pragma unroll
+        for (int k = 0; k < kJRows; ++k) {
+          const int q = q0 + k * rstride;
+          const bool ok = q < x;
+          r[k] = ok ? srho[q] : 0.0;
+          f[k] = ok ? __ldg(reinterpret_cast<const float4*>(rowb + (size_t)q * ld) + v)
+                    : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int k = 0; k < kJRows; ++k) {
+          acc[t][0] = fma((double)f[k].x, r[k], acc[t][0]);
+          acc[t][1] = fma((double)f[k].y, r[k], acc[t][1]);
+          acc[t][2] = fma((double)f[k].z, r[k], acc[t][2]);
+          acc[t][3] = fma((double)f[k].w, r[k], acc[t][3]);
+        }
       }
     }
   }
+  // sum the lane groups of the warp (lanes with equal gl)
+  for (int off = L; off < 32; off <<= 1)
 #pragma unroll
-  for (int t = 0; t < kJMaxVec; ++t) {
-    const int v = lane + 32 * t;
-    if (v < nvec) {
+    for (int t = 0; t < kJMaxVec; ++t)
 #pragma unroll
-      for (int e = 0; e < 4; ++e) part[warp * ld + 4 * v + e] = acc[t][e];
+      for (int e = 0; e < 4; ++e) acc[t][e] += __shfl_xor_sync(0xffffffffu, acc[t][e], off);
+  if (grp == 0) {
+#pragma unroll
+    for (int t = 0; t < kJMaxVec; ++t) {
+      const int v = gl + L * t;
+      if (v < nvec) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) part[warp * ld + 4 * v + e] = acc[t][e];
+      }
     }
   }
   __syncthreads();
@@ -70,12 +101,13 @@ __global__ void __launch_bounds__(kJThreads)
 
 // Fitted density rho[mol][Q] = sum_{mu,nu} B[mu][Q][nu] D[mu][nu] (D symmetric),
 // read from the nu <= mu half with weights 2 (nu < mu) and 1 (nu = mu).
-// Stage 1: one CTA per (molecule, mu), shaped like the Coulomb kernel (8
-// warps split the Q rows, lanes read float4 along nu against the weighted
-// density row staged in shared memory), writes the row partial
-// part[mol][mu][Q] (FP64, warp-shuffle sums).  Stage 2 adds the partials over
-// mu in a fixed order, so the result is deterministic.  Reference:
-// rho = B^T vec(D) of src/scf/cuda/df_coulomb.cpp:38-57 (FP64 cublasDgemv).
+// Stage 1: one CTA per (molecule, mu), shaped like the Coulomb kernel (lane
+// groups sized to the row, kJRows independent Q rows per group and pass,
+// weighted density row staged in shared memory), writes the row partial
+// part[mol][mu][Q] (FP64, shuffle sums within the group).  Stage 2 adds the
+// partials over mu in a fixed order, so the result is deterministic.
+// Reference: rho = B^T vec(D) of src/scf/cuda/df_coulomb.cpp:38-57 (FP64
+// cublasDgemv).
 __global__ void __launch_bounds__(kJThreads)
     fitted_rows_fp32_kernel(const float* __restrict__ b, const double* __restrict__ d, int n,
                             int x, int ld, double* __restrict__ part) {
@@ -88,20 +120,41 @@ __global__ void __launch_bounds__(kJThreads)
   __syncthreads();
   const float* rowb = b + ((size_t)mol * n + mu) * (size_t)x * ld;
   const int nvec = (mu + 1 + 3) / 4;
+  const int L = group_lanes(nvec), G = 32 / L, grp = lane / L, gl = lane % L;
+  const int rstride = kJWarps * G;
   double* out = part + ((size_t)mol * n + mu) * x;
-  for (int q = warp; q < x; q += kJWarps) {
-    const float4* p4 = reinterpret_cast<const float4*>(rowb + (size_t)q * ld);
-    double acc = 0.0;
-    for (int v = lane; v < nvec; v += 32) {
-      const float4 f = __ldg(p4 + v);
-      const double* w = sw + 4 * v;
-      acc = fma((double)f.x, w[0], acc);
-      acc = fma((double)f.y, w[1], acc);
-      acc = fma((double)f.z, w[2], acc);
-      acc = fma((double)f.w, w[3], acc);
+  for (int q0 = warp * G + grp; q0 - grp < x; q0 += kJRows * rstride) {  // warp-uniform trips
+    double acc[kJRows];
+#pragma unroll
+    for (int k = 0; k < kJRows; ++k) acc[k] = 0.0;
+#pragma unroll
+    for (int t = 0; t < kJMaxVec; ++t) {
+      const int v = gl + L * t;
+      if (v < nvec) {
+        const double w0 = sw[4 * v], w1 = sw[4 * v + 1], w2 = sw[4 * v + 2], w3 = sw[4 * v + 3];
+        float4 f[kJRows];
+#pragma unroll
+        for (int k = 0; k < kJRows; ++k) {
+          const int q = q0 + k * rstride;
+          f[k] = q < x ? __ldg(reinterpret_cast<const float4*>(rowb + (size_t)q * ld) + v)
+                       : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int k = 0; k < kJRows; ++k) {
+          acc[k] = fma((double)f[k].x, w0, acc[k]);
+          acc[k] = fma((double)f[k].y, w1, acc[k]);
+          acc[k] = fma((double)f[k].z, w2, acc[k]);
+          acc[k] = fma((double)f[k].w, w3, acc[k]);
+        }
+      }
     }
-    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
-    if (lane == 0) out[q] = acc;
+#pragma unroll
+    for (int k = 0; k < kJRows; ++k) {
+      double sum = acc[k];
+      for (int off = L >> 1; off > 0; off >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, off, L);
+      const int q = q0 + k * rstride;
+      if (gl == 0 && q < x) out[q] = sum;
+    }
   }
 }
 
@@ -219,7 +272,7 @@ extern "C" int vqc_fitted_density_fp32(const float* b_aux_major, const double* d
                                        int32_t nao, int32_t ld_ao, int32_t naux, double* partial,
                                        double* rho, void* stream) {
   if (!b_aux_major || !dens || !partial || !rho || nmol <= 0 || nao <= 0 || naux <= 0 ||
-      ld_ao < nao || ld_ao % 4 || nmol > 65535 || nao > 0x7fffffff / 2)
+      ld_ao < nao || ld_ao % 4 || ld_ao > 4 * 32 * kJMaxVec || nmol > 65535)
     return fail(VQC_STATUS_INVALID_ARGUMENT, "fitted_density_fp32: bad argument");
   const size_t smem = (size_t)ld_ao * sizeof(double);
   if (smem > 48 * 1024) return fail(VQC_STATUS_INVALID_ARGUMENT, "fitted_density_fp32: nao too large");

@@ -141,10 +141,13 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// Round a finite FP32 value to the nearest TF32 value (10 mantissa bits),
+// ties away from zero: add half of the dropped 13-bit field to the
+// sign-magnitude bit pattern (a carry moves into the exponent as it should)
+// and clear the field.  Two integer ops on the full-rate ALUs instead of the
+// narrower conversion pipe; same result as cvt.rna.tf32.f32 for finite x.
 __device__ __forceinline__ float rn_tf32(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return __uint_as_float(r);
+  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
 }
 
 __device__ __forceinline__ void split4(float4& v, float4& lo) {
@@ -282,8 +285,10 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
     for (int item = i0; item < i1; ++item) {
       for (int kb = 0; kb < nk; ++kb, ++g) {
         const int s = g % S;
-        if (!mbar_wait(full0 + 8 * s, (g / S) & 1, ab)) {
-          set_abort(ctrl, p.error, 12);
+        // every lane waits; the warp leaves together (no lane may skip a
+        // later warp-collective alone)
+        if (!__all_sync(0xffffffffu, mbar_wait(full0 + 8 * s, (g / S) & 1, ab))) {
+          if (lane == 0) set_abort(ctrl, p.error, 12);
           goto split_done;
         }
         if (ts == 0) *reinterpret_cast<volatile int*>(&ctrl->consumed) = g + 1;
@@ -363,8 +368,8 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
         rho_acc = 0.0;
         rho_key = key;
       }
-      if (!mbar_wait(af0 + 8 * b, (t >> 1) & 1, ab)) {
-        set_abort(ctrl, p.error, 15);
+      if (!__all_sync(0xffffffffu, mbar_wait(af0 + 8 * b, (t >> 1) & 1, ab))) {
+        if (lane == 0) set_abort(ctrl, p.error, 15);
         break;
       }
       fence_after_sync();
@@ -575,8 +580,8 @@ __global__ void __launch_bounds__(kGramThreads, 1)
     const int q = warp & 3, half = (warp - 2) >> 2;
     for (int ch = 0; ch < nchains; ++ch) {
       const int b = ch & 1;
-      if (!mbar_wait(af0 + 8 * b, (ch >> 1) & 1, ab)) {
-        set_abort(ctrl, p.error, 24);
+      if (!__all_sync(0xffffffffu, mbar_wait(af0 + 8 * b, (ch >> 1) & 1, ab))) {
+        if (lane == 0) set_abort(ctrl, p.error, 24);
         break;
       }
       fence_after_sync();

@@ -136,6 +136,8 @@ class MixedBuilder:
         self.o_pad = _round_up(nocc, 16)
         if self.o_pad > 128:
             raise _lib.VqcError(1, "mixed exchange supports at most 128 occupied orbitals")
+        if self.ld > 512:
+            raise _lib.VqcError(1, "mixed J/K support at most 512 orbital basis functions")
         dev = b_packed.device
         self.b = torch.empty(nb, n, x, self.ld, dtype=torch.float32, device=dev)
         self.st = torch.cuda.current_stream().cuda_stream

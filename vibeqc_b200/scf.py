@@ -15,6 +15,8 @@ max|FDS - SDF| <= 10 * min(1e-8, density_tolerance)
 
 from __future__ import annotations
 
+import os
+
 import math
 from dataclasses import dataclass, field
 
@@ -212,6 +214,9 @@ class _SP2Graph:
         self.xn = torch.empty_like(self.x)
         self.done = torch.zeros(nb, dtype=torch.int32, device=device)
         self.args = (nb, n, float(nocc), float(tol))
+        self.graph = None
+        if os.environ.get("VQC_SP2_GRAPHS", "1") == "0":
+            return  # eager launches (e.g. under a kernel profiler)
         side = torch.cuda.Stream(device=device)
         side.wait_stream(torch.cuda.current_stream(device))
         with torch.cuda.stream(side):  # warm-up outside capture (cuBLAS handles, workspaces)
@@ -219,6 +224,14 @@ class _SP2Graph:
         torch.cuda.current_stream(device).wait_stream(side)
         self.graph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(self.graph):
+            self._steps()
+
+    def run(self):
+        """SP2_GRAPH_STEPS steps: one graph replay, or eager launches."""
+        if self.graph is not None:
+            self.graph.replay()
+            GRAPH_LAUNCHES[0] += SP2_GRAPH_STEPS
+        else:
             self._steps()
 
     def _steps(self):
@@ -268,8 +281,7 @@ def purify_sp2(fo: torch.Tensor, nocc: int, max_steps: int = 96, tol: float = 1e
     torch.div(emax[:, None, None] * eye - fo, (emax - emin)[:, None, None], out=g.x)
     g.done.zero_()
     for _ in range(0, max_steps, SP2_GRAPH_STEPS):
-        g.graph.replay()
-        GRAPH_LAUNCHES[0] += SP2_GRAPH_STEPS
+        g.run()
         if bool(g.done.all()):
             break
     return 0.5 * (g.x + g.x.transpose(1, 2))
