@@ -11,11 +11,12 @@
 //     (reference src/scf/cuda/df_occupied_exchange.cpp:251-257).  Persistent
 //     over (mu, 128-row Q tile) items; each CTA takes a contiguous item range
 //     with mu fastest, so rho rows accumulate in registers across items.  U is
-//     written as [mol][mu][i][Q] (Q contiguous: coalesced epilogue stores).  Warp roles: one TMA producer, four
-//     splitter warps that split the streamed FP32 B tile (hi in place, lo in a
-//     sibling buffer), one MMA-issuing thread, four epilogue warps.  C arrives
-//     pre-split.  Two TMEM accumulators let an item's epilogue (U written
-//     already split, rho[Q] += 2 sum_i U C[mu][i] for J) overlap the next
+//     written as [mol][mu][i][Q] (Q contiguous: coalesced epilogue stores).
+//     Warp roles: one TMA producer, eight splitter warps that split the
+//     streamed FP32 B tile (hi in place, lo in a sibling buffer), one
+//     MMA-issuing thread, eight epilogue warps (two per TMEM lane quarter).
+//     C arrives pre-split.  Two TMEM accumulators let an item's epilogue (U
+//     written already split, rho[Q] += 2 sum_i U C[mu][i] for J) overlap the next
 //     item's MMAs.  The kernel streams B once: HBM-bound by design.
 //   gram_ws_kernel -- K[mol] += U U^T over kdim = X * o_pad (reference
 //     df_occupied_exchange.cpp:262-279) from the pre-split U: a pure
@@ -185,11 +186,17 @@ __device__ __forceinline__ bool aborted(Ctrl* c) {
 // ---------------------------------------------------------------------------
 // half transform: U[z][Q][i] = sum_nu B[z][Q][nu] C[mol(z)][i][nu], 3xTF32,
 // persistent over (z, 128-row Q tile) items; warp roles:
-//   w0 TMA producer, w1-w4 splitters (A -> hi in place + lo), w5 MMA issuer,
-//   w6-w9 epilogue (TMEM -> U hi/lo in HBM, rho partial sums)
+//   w0 TMA producer, w1-w8 splitters (A -> hi in place + lo), w9 MMA issuer,
+//   w10-w17 epilogue (TMEM -> U hi/lo in HBM, rho partial sums)
 // ---------------------------------------------------------------------------
 
-constexpr int kHalfThreads = 320;
+// warps: 0 TMA producer, 1-8 splitters, 9 MMA issuer, 10-17 epilogue (two per
+// TMEM lane quarter, interleaved 16-column chunks): the split and the
+// TMEM -> HBM epilogue are per-warp latency-bound, so each has eight warps
+constexpr int kHalfThreads = 576;
+constexpr int kSplitWarps = 8;
+constexpr int kMmaWarp = 1 + kSplitWarps;
+constexpr int kEpiWarp0 = kMmaWarp + 1;
 constexpr int kGramThreads = 320;
 constexpr int kTmemBuf = 128;  // columns per accumulator buffer (two buffers)
 
@@ -230,12 +237,12 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
   if (tid == 0) {
     for (int s = 0; s < S; ++s) {
       mbar_init(full0 + 8 * s, 1);
-      mbar_init(conv0 + 8 * s, 4);
+      mbar_init(conv0 + 8 * s, kSplitWarps);
       mbar_init(empty0 + 8 * s, 1);
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(af0 + 8 * b, 1);
-      mbar_init(ae0 + 8 * b, 4);
+      mbar_init(ae0 + 8 * b, 8);
     }
     ctrl->abort = 0;
     ctrl->issued = ctrl->consumed = ctrl->commits = 0;
@@ -278,7 +285,7 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
         }
       }
     }
-  } else if (warp >= 1 && warp <= 4) {  // splitters
+  } else if (warp >= 1 && warp <= kSplitWarps) {  // splitters
     const int ts = tid - 32;
     int g = 0;
     const int i0 = blockIdx.x * p.per_cta, i1 = min(p.nitems, i0 + p.per_cta);
@@ -295,7 +302,7 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
         float4* a = reinterpret_cast<float4*>(stage(s));
         float4* alo = reinterpret_cast<float4*>(stage(s) + C::A_BYTES);
 #pragma unroll 4
-        for (int k = ts; k < C::A_BYTES / 16; k += 128) {
+        for (int k = ts; k < C::A_BYTES / 16; k += 32 * kSplitWarps) {
           float4 v = a[k], lo;
           split4(v, lo);
           a[k] = v;
@@ -307,7 +314,7 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
       }
     }
   split_done:;
-  } else if (warp == 5) {
+  } else if (warp == kMmaWarp) {
     if (lane == 0) {  // MMA issuer
       constexpr uint32_t idesc = instr_desc<BN>();
       int g = 0, t = 0;
@@ -346,8 +353,9 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
         mma_commit(af0 + 8 * b);
       }
     }
-  } else {  // epilogue warps 6..9
+  } else {  // epilogue warps kEpiWarp0 .. kEpiWarp0 + 7
     const int q = warp & 3;  // TMEM lane quarter this warp may access
+    const int half = (warp - kEpiWarp0) >> 2;  // which interleaved 16-column chunks
     int t = 0;
     const int i0 = blockIdx.x * p.per_cta, i1 = min(p.nitems, i0 + p.per_cta);
     double rho_acc = 0.0;
@@ -378,7 +386,7 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
       float* ul = p.u_lo + (size_t)z * p.nocc * p.ldq + row;
       const double* cv = p.cvec + (size_t)z * p.nocc;
 #pragma unroll
-      for (int c = 0; c < BN; c += 16) {
+      for (int c = 16 * half; c < BN; c += 32) {
         float v[16];
         tmem_ld16(tmem + b * kTmemBuf + ((uint32_t)(q * 32) << 16) + c, v);
         if (valid) {
