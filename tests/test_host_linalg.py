@@ -83,20 +83,3 @@ def test_gradient_weights_match_dense_formulas(n, o, x, upper, monkeypatch):
     ref_mbar = -0.5 * torch.outer(cvec, cvec) + gam.reshape(x, -1) @ gam.reshape(x, -1).T
     assert torch.allclose(abar, ref_abar, rtol=0, atol=1e-11 * ref_abar.abs().max().item())
     assert torch.allclose(mbar, ref_mbar, rtol=0, atol=1e-11 * ref_mbar.abs().max().item())
-
-
-def test_packed_half_transform_matches_full(monkeypatch):
-    from vibeqc_b200 import jk
-
-    monkeypatch.setattr(jk, "HALF_BLOCK_BYTES", 8 * 3 * 11 * 17 * 2)  # two AO rows per block
-    g = torch.Generator().manual_seed(2)
-    nb, n, x, o = 3, 11, 17, 4
-    bp = torch.randn(nb, n * (n + 1) // 2, x, dtype=torch.float64, generator=g)
-    c = torch.randn(nb, n, o, dtype=torch.float64, generator=g)
-    full = bp[:, jk.unpack_index(n, "cpu")].view(nb, n, n, x)
-    rho, u = jk.fp64_half_packed(bp, c, n, x)
-    rho_f, u_f = jk.fp64_half(full.reshape(nb, n * n, x), c, n, x)
-    ref = torch.einsum("bmnq,bni->bmiq", full, c)
-    assert torch.allclose(u, ref, atol=1e-12) and torch.allclose(u_f, ref, atol=1e-12)
-    assert torch.allclose(rho, rho_f, atol=1e-11)
-    assert torch.allclose(rho, torch.einsum("bmnq,bmn->bq", full, 2 * c @ c.transpose(1, 2)), atol=1e-10)

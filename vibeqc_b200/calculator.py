@@ -385,10 +385,10 @@ def _device_bytes_per_molecule(nao: int, naux: int, precision: str) -> int:
     """Peak device bytes one molecule holds during a chunk (integrals to gradient)."""
     p = nao * (nao + 1) // 2
     # fp64: full FP64 B (16) + packed A during whitening / packed Abar (8) + K temporaries;
-    # mixed: packed FP64 B (8) + full FP32 B (8) + anchor/increment buffers of
+    # mixed: full FP64 B (16) + full FP32 B (8) + anchor/increment buffers of
     # N*o*X elements (~2o/N * 24 per packed element) + anchor temporaries;
     # the FP32 buffers are released before the packed Abar (8) is formed
-    per_px = 30 if precision == "fp64" else 32
+    per_px = 30 if precision == "fp64" else 40
     return int(per_px * p * naux + 64 * nao * nao)
 
 

@@ -442,7 +442,7 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
 //   TMEM lane quarter; FP64 accumulators drained every kGramFlush K-blocks)
 // ---------------------------------------------------------------------------
 
-constexpr int kGramFlush = 2;
+constexpr int kGramFlush = 4;  // K-blocks per FP32 TMEM chain before the FP64 drain (48 accumulation steps)
 
 struct GramCfg {
   static constexpr int TILE = BM * BK * 4;  // 16 KB

@@ -329,8 +329,12 @@ def whiten_in_place(a: torch.Tensor, mf: MetricFactor) -> None:
     """
     nb, p_rows, x = a.shape
     w = mf.inv_sqrt
-    blk = max(256, (1 << 28) // (8 * x * nb))  # ~256 MB of rows per step
     cb = WHITEN_COLUMN_BLOCK
+    # rows are views; only the (nb, blk, cb) product block is a temporary
+    # (~512 MB), so the GEMMs are tall enough to run near the FP64 peak
+    blk = max(256, (1 << 29) // (8 * max(cb, 1) * nb))
+    if mf.kind != "cholesky":
+        blk = max(256, (1 << 29) // (8 * x * nb))
     for r0 in range(0, p_rows, blk):
         rows = a[:, r0:r0 + blk]
         if mf.kind != "cholesky":
@@ -398,6 +402,7 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
     def density_from(f, guess, tol=1e-11, noise_scale=0.3):
         with TIMER.stage("purify"):
             proj = purify_sp2(xo.transpose(1, 2) @ f @ xo, nocc, tol=tol, graphs=sp2_graphs)
+        with TIMER.stage("occupied_factor"):
             co = occupied_factor(proj, guess, gen, noise_scale)  # orthonormal, orthogonal basis
         return 2.0 * (xo @ proj @ xo.transpose(1, 2)), co
 
