@@ -22,6 +22,18 @@ import torch
 from .timing import TIMER
 
 
+# algorithmic work of the tensor-core exchange since the last reset (host-side
+# tallies, read by the benchmark): bytes the half transform must move (FP32 B
+# read once, split U written), its launches, and the exchange flops counted
+# once (half transform 2 N^2 X o, Gram X o N (N + 1) per term)
+COUNTERS = {"half_bytes": 0, "half_launches": 0, "k_flops": 0}
+
+
+def reset_counters() -> None:
+    for k in COUNTERS:
+        COUNTERS[k] = 0
+
+
 def unpack_index(n: int, device) -> torch.Tensor:
     mu = torch.arange(n, device=device)
     hi = torch.maximum(mu[:, None], mu[None, :])
@@ -133,6 +145,9 @@ class MixedBuilder:
         self._lib.call("vqc_split_tf32", ct.data_ptr(), ct_hi.data_ptr(), ct_lo.data_ptr(),
                        ct.numel(), self.st)
         c64 = (c_occ if cvec is None else cvec).contiguous()
+        COUNTERS["half_bytes"] += nb * n * self.x * self.ld * 4 + nb * n * o * self.ldq * 8
+        COUNTERS["half_launches"] += 1
+        COUNTERS["k_flops"] += 2 * nb * n * n * self.x * o
         with TIMER.stage("K_half_tc"):
             self._lib.call("vqc_tc_half_transform", self.b.data_ptr(), nb, n, self.ld, self.x,
                            ct_hi.data_ptr(), ct_lo.data_ptr(), c64.data_ptr(), o, self.o_pad,
@@ -152,6 +167,7 @@ class MixedBuilder:
             self._lib.call("vqc_coulomb_fp32", self.b.data_ptr(), self.rho.data_ptr(), nb, n,
                            self.ld, self.x, j.data_ptr(), self.st)
         k = torch.zeros(nb, n, n, dtype=torch.float64, device=d.device)
+        COUNTERS["k_flops"] += nb * self.x * self.nocc * n * (n + 1)
         with TIMER.stage("K_gram_tc"):
             self._lib.call("vqc_tc_gram", self.u_hi.data_ptr(), self.u_lo.data_ptr(), nb, n,
                            self.nocc * self.ldq, k.data_ptr(), self.err.data_ptr(), self.st)
@@ -210,6 +226,7 @@ class MixedBuilder:
         with TIMER.stage("J_fp32"):
             self._lib.call("vqc_coulomb_fp32", self.b.data_ptr(), drho.data_ptr(), nb, n,
                            self.ld, x, dj.data_ptr(), self.st)
+        COUNTERS["k_flops"] += 2 * nb * x * o * n * (n + 1)  # V dU^T + dU V^T
         with TIMER.stage("K_gram_tc"):
             self._lib.call("vqc_anchor_combine", self.u0.data_ptr(), self.u_hi.data_ptr(),
                            self.u_lo.data_ptr(), self.v_hi.data_ptr(), self.v_lo.data_ptr(),
