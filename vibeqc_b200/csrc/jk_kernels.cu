@@ -27,6 +27,9 @@ __device__ __forceinline__ int group_lanes(int nvec) {
   return l;
 }
 
+// MV = float4 columns per lane (rows up to 128 * MV): the accumulators scale
+// with the row length, so short rows keep registers (and occupancy) low
+template <int MV>
 __global__ void __launch_bounds__(kJThreads)
     coulomb_fp32_kernel(const float* __restrict__ b, const double* __restrict__ rho, int n, int x,
                         int ld, double* __restrict__ j) {
@@ -41,15 +44,15 @@ __global__ void __launch_bounds__(kJThreads)
   const int nvec = (mu + 1 + 3) / 4;  // float4 columns covering nu <= mu (ld % 4 == 0)
   const int L = group_lanes(nvec), G = 32 / L, grp = lane / L, gl = lane % L;
   const int rstride = kJWarps * G;  // lane groups per CTA
-  double acc[kJMaxVec][4];
+  double acc[MV][4];
 #pragma unroll
-  for (int t = 0; t < kJMaxVec; ++t)
+  for (int t = 0; t < MV; ++t)
 #pragma unroll
     for (int e = 0; e < 4; ++e) acc[t][e] = 0.0;
   // q0 - grp is the same for every lane of the warp: the trip count is uniform
   for (int q0 = warp * G + grp; q0 - grp < x; q0 += kJRows * rstride) {
 #pragma unroll
-    for (int t = 0; t < kJMaxVec; ++t) {
+    for (int t = 0; t < MV; ++t) {
       const int v = gl + L * t;
       if (v < nvec) {
         float4 f[kJRows];
@@ -75,12 +78,12 @@ __global__ void __launch_bounds__(kJThreads)
   // sum the lane groups of the warp (lanes with equal gl)
   for (int off = L; off < 32; off <<= 1)
 #pragma unroll
-    for (int t = 0; t < kJMaxVec; ++t)
+    for (int t = 0; t < MV; ++t)
 #pragma unroll
       for (int e = 0; e < 4; ++e) acc[t][e] += __shfl_xor_sync(0xffffffffu, acc[t][e], off);
   if (grp == 0) {
 #pragma unroll
-    for (int t = 0; t < kJMaxVec; ++t) {
+    for (int t = 0; t < MV; ++t) {
       const int v = gl + L * t;
       if (v < nvec) {
 #pragma unroll
@@ -108,6 +111,7 @@ __global__ void __launch_bounds__(kJThreads)
 // partials over mu in a fixed order, so the result is deterministic.
 // Reference: rho = B^T vec(D) of src/scf/cuda/df_coulomb.cpp:38-57 (FP64
 // cublasDgemv).
+template <int MV>
 __global__ void __launch_bounds__(kJThreads)
     fitted_rows_fp32_kernel(const float* __restrict__ b, const double* __restrict__ d, int n,
                             int x, int ld, double* __restrict__ part) {
@@ -128,7 +132,7 @@ __global__ void __launch_bounds__(kJThreads)
 #pragma unroll
     for (int k = 0; k < kJRows; ++k) acc[k] = 0.0;
 #pragma unroll
-    for (int t = 0; t < kJMaxVec; ++t) {
+    for (int t = 0; t < MV; ++t) {
       const int v = gl + L * t;
       if (v < nvec) {
         const double w0 = sw[4 * v], w1 = sw[4 * v + 1], w2 = sw[4 * v + 2], w3 = sw[4 * v + 3];
@@ -256,14 +260,17 @@ extern "C" int vqc_coulomb_fp32(const float* b_aux_major, const double* rho, int
     return fail(VQC_STATUS_INVALID_ARGUMENT, "coulomb_fp32: bad argument");
   const size_t smem = ((size_t)((naux + 1) & ~1) + (size_t)kJWarps * ld_ao) * sizeof(double);
   if (smem > 200 * 1024) return fail(VQC_STATUS_INVALID_ARGUMENT, "coulomb_fp32: too many auxiliary functions");
+  dim3 grid(nao, nmol);
+  const int mv = (ld_ao / 4 + 31) / 32;
+  auto kern = mv <= 1 ? coulomb_fp32_kernel<1>
+              : mv == 2 ? coulomb_fp32_kernel<2>
+              : mv == 3 ? coulomb_fp32_kernel<3>
+                        : coulomb_fp32_kernel<4>;
   if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(coulomb_fp32_kernel,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return cuda_status(e, "coulomb_fp32 smem");
   }
-  dim3 grid(nao, nmol);
-  coulomb_fp32_kernel<<<grid, kJThreads, smem, (cudaStream_t)stream>>>(b_aux_major, rho, nao, naux,
-                                                                        ld_ao, j);
+  kern<<<grid, kJThreads, smem, (cudaStream_t)stream>>>(b_aux_major, rho, nao, naux, ld_ao, j);
   count_launch();
   return cuda_status(cudaGetLastError(), "coulomb_fp32");
 }
@@ -277,8 +284,12 @@ extern "C" int vqc_fitted_density_fp32(const float* b_aux_major, const double* d
   const size_t smem = (size_t)ld_ao * sizeof(double);
   if (smem > 48 * 1024) return fail(VQC_STATUS_INVALID_ARGUMENT, "fitted_density_fp32: nao too large");
   dim3 g1(nao, nmol);
-  fitted_rows_fp32_kernel<<<g1, kJThreads, smem, (cudaStream_t)stream>>>(b_aux_major, dens, nao,
-                                                                         naux, ld_ao, partial);
+  const int mv = (ld_ao / 4 + 31) / 32;
+  auto kern = mv <= 1 ? fitted_rows_fp32_kernel<1>
+              : mv == 2 ? fitted_rows_fp32_kernel<2>
+              : mv == 3 ? fitted_rows_fp32_kernel<3>
+                        : fitted_rows_fp32_kernel<4>;
+  kern<<<g1, kJThreads, smem, (cudaStream_t)stream>>>(b_aux_major, dens, nao, naux, ld_ao, partial);
   count_launch();
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_status(e, "fitted_density_fp32 rows");
