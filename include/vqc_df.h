@@ -175,6 +175,11 @@ int vqc_sp2_update(const double* x, const double* x2, double* xout, int32_t nmol
 int vqc_unpack_aux_major(const double* b_packed, int32_t nmol, int32_t nao, int32_t naux,
                          int32_t ld_ao, float* b_aux_major, void* stream);
 int vqc_split_tf32(const float* x, float* hi, float* lo, int64_t n, void* stream);
+/* Self-test of the tensor-core kernels' bounded waits: a one-warp kernel waits
+ * on a barrier that nothing completes, gives up after budget_us microseconds
+ * (<= 2 s) and writes 31 to *error; the context stays usable.  No counterpart
+ * in the reference. */
+int vqc_wait_selftest(int32_t budget_us, int32_t* error, void* stream);
 int vqc_tc_half_transform(const float* b_aux_major, int32_t nmol, int32_t nao, int32_t ld_ao,
                           int32_t naux, const float* ct_hi, const float* ct_lo,
                           const double* c_occ, int32_t nocc, int32_t o_pad, int32_t ld_aux,

@@ -91,6 +91,7 @@ _SIGNATURES = {
     "vqc_unpack_aux_major": ([_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                               ctypes.c_int32, _P, _P], ctypes.c_int),
     "vqc_split_tf32": ([_P, _P, _P, ctypes.c_int64, _P], ctypes.c_int),
+    "vqc_wait_selftest": ([ctypes.c_int32, _P, _P], ctypes.c_int),
     "vqc_tc_half_transform": ([_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                ctypes.c_int32, _P, _P, _P, ctypes.c_int32, ctypes.c_int32,
                                ctypes.c_int32, _P, _P, _P, _P, _P], ctypes.c_int),

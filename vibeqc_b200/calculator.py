@@ -332,11 +332,15 @@ class PreparedBatch:
         dev = calc.device
         with torch.cuda.device(dev):
             for bucket, chunk in enumerate(self._chunks):
-                xyz_h = np.concatenate([coords[i] for i in chunk.indices], axis=0)
-                if not np.isfinite(xyz_h).all():
+                # an item with non-finite coordinates fails alone: its slot in
+                # the chunk computes the prepared geometry, its peers continue
+                bad = {i for i in chunk.indices if not np.isfinite(coords[i]).all()}
+                if len(bad) == len(chunk.indices):
                     for i in chunk.indices:
                         items[i] = _failed(i, bucket, STATUS_INVALID_ARGUMENT, "non-finite coordinates")
                     continue
+                xyz_h = np.concatenate([self._molecules[i].coordinates if i in bad else coords[i]
+                                        for i in chunk.indices], axis=0)
                 xyz = torch.as_tensor(xyz_h, dtype=torch.float64).to(dev, non_blocking=True)
                 try:
                     out, grad = self._run_chunk(chunk, xyz, want_forces)
@@ -356,6 +360,9 @@ class PreparedBatch:
                     na = self._natoms[i]
                     forces = None if g is None else -g[off:off + na].copy()
                     off += na
+                    if i in bad:
+                        items[i] = _failed(i, bucket, STATUS_INVALID_ARGUMENT, "non-finite coordinates")
+                        continue
                     ok = bool(conv[j])
                     items[i] = BatchItemResult(
                         index=i,

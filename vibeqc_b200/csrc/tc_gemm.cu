@@ -65,8 +65,9 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
                : "memory");
 }
 
-// bounded wait; false on timeout or when *abort is set
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort) {
+// bounded wait; false on timeout (budget_ns of %globaltimer) or when *abort is set
+__device__ __forceinline__ bool mbar_wait_for(uint32_t bar, uint32_t parity, volatile int* abort,
+                                              unsigned long long budget_ns) {
   const unsigned long long t0 = globaltimer();
   while (true) {
     uint32_t ok;
@@ -79,8 +80,12 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatil
         : "memory");
     if (ok) return true;
     if (*abort) return false;
-    if (globaltimer() - t0 > kWaitNs) return false;
+    if (globaltimer() - t0 > budget_ns) return false;
   }
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort) {
+  return mbar_wait_for(bar, parity, abort, kWaitNs);
 }
 
 __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* tm, int c0, int c1,
@@ -641,6 +646,24 @@ __global__ void __launch_bounds__(kGramThreads, 1)
   }
 }
 
+// Self-test of the bounded-wait error path: one warp waits on an mbarrier
+// that nothing ever arrives on; the wait must give up after budget_ns and
+// the kernel must report it in *error and return normally.
+constexpr int kWaitSelftestCode = 31;
+
+__global__ void wait_selftest_kernel(unsigned long long budget_ns, int* error) {
+  __shared__ uint64_t bar;
+  __shared__ int never;
+  if (threadIdx.x == 0) {
+    mbar_init(smem_u32(&bar), 1);
+    never = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncwarp();
+  const bool ok = mbar_wait_for(smem_u32(&bar), 0, &never, budget_ns);
+  if (!__all_sync(0xffffffffu, ok) && threadIdx.x == 0) atomicExch(error, kWaitSelftestCode);
+}
+
 __global__ void split_tf32_kernel(const float* __restrict__ x, float* __restrict__ hi,
                                   float* __restrict__ lo, size_t n) {
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -714,6 +737,15 @@ static int launch_half(const CUtensorMap& ta, const CUtensorMap& th, const CUten
 
 using namespace vqc;
 using namespace vqc::tc;
+
+extern "C" int vqc_wait_selftest(int32_t budget_us, int32_t* error, void* stream) {
+  if (!error || budget_us <= 0 || budget_us > 2000000)
+    return fail(VQC_STATUS_INVALID_ARGUMENT, "wait_selftest: budget must be in (0, 2 s]");
+  wait_selftest_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(1000ull * (unsigned long long)budget_us,
+                                                          error);
+  count_launch();
+  return cuda_status(cudaGetLastError(), "wait_selftest");
+}
 
 extern "C" int vqc_split_tf32(const float* x, float* hi, float* lo, int64_t n, void* stream) {
   if (!x || !hi || !lo || n < 0) return fail(VQC_STATUS_INVALID_ARGUMENT, "split_tf32: bad argument");
