@@ -109,7 +109,8 @@ __host__ __device__ constexpr int round32(int n) { return (n + 31) / 32 * 32; }
 // ---------------------------------------------------------------------------
 
 template <int LA, int LB, int LC, bool SPH>
-__global__ void __launch_bounds__(round32(Int3cCfg<LA, LB, LC, SPH>::THREADS))
+__global__ void __launch_bounds__(round32(Int3cCfg<LA, LB, LC, SPH>::THREADS),
+                                  min_ctas_grad3c(LA, LB, LC))
     grad3c_kernel(DevBasis orb, DevBasis aux, const double* __restrict__ xyz,
                   const DevMol* __restrict__ mols, const int2* __restrict__ pairs,
                   const ClassMol* __restrict__ cms, int ncm, const double* __restrict__ abar,

@@ -69,7 +69,7 @@ __device__ __forceinline__ void transform_ab(int mode, const double (&acc)[ncart
 // ---------------------------------------------------------------------------
 
 template <int LA, int LB, int LC, bool SPH>
-__global__ void __launch_bounds__(Int3cCfg<LA, LB, LC, SPH>::THREADS)
+__global__ void __launch_bounds__(Int3cCfg<LA, LB, LC, SPH>::THREADS, min_ctas3c(LA, LB, LC))
     int3c_kernel(DevBasis orb, DevBasis aux, const double* __restrict__ xyz,
                  const DevMol* __restrict__ mols, const int2* __restrict__ pairs,
                  const ClassMol* __restrict__ cms, int ncm, double* __restrict__ out) {

@@ -47,6 +47,19 @@ __host__ __device__ constexpr int slots3c(int la, int lb, int lc, bool sph) {
              : (5120 / (ncart(lc) * out_count(la, sph) * out_count(lb, sph)));
 }
 
+// Resident CTAs per SM requested from the compiler for the 3-centre kernels:
+// the low-l classes (the most frequent and the most contracted) are latency-
+// bound on FP64 dependencies at one or two CTAs, so they are compiled to fit
+// more (fewer registers, a few hundred bytes of spills); the high-l classes
+// keep their registers.  Measured on 48 clusters: values 127 -> 79 ms,
+// derivatives 171 -> 128 ms per step.
+__host__ __device__ constexpr int min_ctas3c(int la, int lb, int lc) {
+  return la + lb + lc <= 3 ? 3 : (la + lb + lc <= 5 ? 2 : 1);
+}
+__host__ __device__ constexpr int min_ctas_grad3c(int la, int lb, int lc) {
+  return la + lb + lc <= 5 ? 2 : 1;
+}
+
 template <int LA, int LB, int LC, bool SPH>
 struct Int3cCfg {
   static constexpr int NOA = out_count(LA, SPH), NOB = out_count(LB, SPH), NOC = out_count(LC, SPH);
