@@ -67,9 +67,6 @@ class FP64Builder:
         self.nbuild += 1
         return j, k
 
-    def whitened_fp64(self) -> torch.Tensor:
-        return self.b
-
     def build_exact(self, d: torch.Tensor, c_occ: torch.Tensor):
         return self.build(d, c_occ)
 
