@@ -46,3 +46,19 @@ def test_mixed_matches_fp64_and_reference(name):
     assert np.abs(fmx - f64).max() <= 1e-5
     assert abs(emx - case["energy"]) <= 1e-6
     assert np.abs(fmx - np.array(case["forces"])).max() <= 1e-5
+
+
+def test_decane_mixed_matches_fp64():
+    """Single all-trans n-decane, def2-SVP (250 AO), FP64 vs mixed on the GPU.
+
+    No carbon JK-fit set is bundled; def2-TZVP (442 functions) stands in as the
+    auxiliary basis, fed identically to both precisions.
+    """
+    from vibeqc_b200 import geometry
+
+    mol = make_molecule(geometry.alkane(10, 0), "def2-svp", "def2-tzvp")
+    e64, f64, c64 = _run(mol, "fp64")
+    emx, fmx, cmx = _run(mol, "mixed")
+    assert c64 and cmx
+    assert abs(emx - e64) <= 1e-6
+    assert np.abs(fmx - f64).max() <= 1e-5

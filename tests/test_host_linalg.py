@@ -65,21 +65,23 @@ def test_gradient_weights_match_dense_formulas(n, o, x, upper, monkeypatch):
     monkeypatch.setattr(gr, "WEIGHT_ROW_BLOCK", 8)
     monkeypatch.setattr(gr, "SYM_BLOCK", 64)
     g = torch.Generator().manual_seed(n)
-    c = torch.randn(n, o, dtype=torch.float64, generator=g)
-    dens = 2.0 * c @ c.T
-    rho = torch.randn(x, dtype=torch.float64, generator=g)
-    u = torch.randn(n, o, x, dtype=torch.float64, generator=g)
-    w = torch.randn(x, x, dtype=torch.float64, generator=g)
+    nb = 2
+    c = torch.randn(nb, n, o, dtype=torch.float64, generator=g)
+    dens = 2.0 * c @ c.transpose(1, 2)
+    rho = torch.randn(nb, x, dtype=torch.float64, generator=g)
+    u = torch.randn(nb, n, o, x, dtype=torch.float64, generator=g)
+    w = torch.randn(nb, x, x, dtype=torch.float64, generator=g)
     if upper:
         w = torch.triu(w)
-    abar, mbar = gr.molecule_weights(c, dens, rho, u, w, upper)
-    # dense restatement: Abar = D (x) cvec - 2 C Gamma C^T, Mbar = -cc^T/2 + Gamma Gamma^T
-    cvec = w @ rho
-    bij = torch.einsum("mi,mjq->qij", c, u)
-    gam = (w @ bij.reshape(x, o * o)).view(x, o, o)
-    full = dens[:, :, None] * cvec - 2.0 * torch.einsum("mi,nj,pij->mnp", c, c, gam)
+    abar, mbar = gr.chunk_weights(c, dens, rho, u, w, upper)
     mu, nu = torch.tril_indices(n, n)
-    ref_abar = full[mu, nu]
-    ref_mbar = -0.5 * torch.outer(cvec, cvec) + gam.reshape(x, -1) @ gam.reshape(x, -1).T
-    assert torch.allclose(abar, ref_abar, rtol=0, atol=1e-11 * ref_abar.abs().max().item())
-    assert torch.allclose(mbar, ref_mbar, rtol=0, atol=1e-11 * ref_mbar.abs().max().item())
+    for m in range(nb):
+        # dense restatement: Abar = D (x) cvec - 2 C Gamma C^T, Mbar = -cc^T/2 + Gamma Gamma^T
+        cvec = w[m] @ rho[m]
+        bij = torch.einsum("mi,mjq->qij", c[m], u[m])
+        gam = (w[m] @ bij.reshape(x, o * o)).view(x, o, o)
+        full = dens[m][:, :, None] * cvec - 2.0 * torch.einsum("mi,nj,pij->mnp", c[m], c[m], gam)
+        ref_abar = full[mu, nu]
+        ref_mbar = -0.5 * torch.outer(cvec, cvec) + gam.reshape(x, -1) @ gam.reshape(x, -1).T
+        assert torch.allclose(abar[m], ref_abar, rtol=0, atol=1e-11 * ref_abar.abs().max().item())
+        assert torch.allclose(mbar[m], ref_mbar, rtol=0, atol=1e-11 * ref_mbar.abs().max().item())

@@ -32,25 +32,23 @@ SYM_BLOCK = 256  # row block of the triangular and symmetric products
 
 
 def _upper_times(w: torch.Tensor, g: torch.Tensor) -> torch.Tensor:
-    """W @ g for upper-triangular W (X, X): row block r needs rows >= r0 of g."""
-    x = w.shape[0]
-    out = torch.empty(x, g.shape[1], dtype=g.dtype, device=g.device)
+    """W @ g per molecule for upper-triangular W (b, X, X): row block r needs rows >= r0 of g."""
+    x = w.shape[1]
+    out = torch.empty(g.shape[0], x, g.shape[2], dtype=g.dtype, device=g.device)
     for r0 in range(0, x, SYM_BLOCK):
         r1 = min(x, r0 + SYM_BLOCK)
-        torch.mm(w[r0:r1, r0:], g[r0:], out=out[r0:r1])
+        out[:, r0:r1] = torch.bmm(w[:, r0:r1, r0:], g[:, r0:])
     return out
 
 
-def _sym_gram(g: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
-    """g g^T from its upper block triangle (mirrored)."""
-    x = g.shape[0]
-    if out is None:
-        out = torch.empty(x, x, dtype=g.dtype, device=g.device)
+def _sym_gram(g: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
+    """g g^T per molecule from the upper block triangle (mirrored)."""
+    x = g.shape[1]
     for r0 in range(0, x, SYM_BLOCK):
         r1 = min(x, r0 + SYM_BLOCK)
-        blk = g[r0:r1] @ g[r0:].T
-        out[r0:r1, r0:] = blk
-        out[r1:, r0:r1] = blk[:, r1 - r0:].T
+        blk = torch.bmm(g[:, r0:r1], g[:, r0:].transpose(1, 2))
+        out[:, r0:r1, r0:] = blk
+        out[:, r1:, r0:r1] = blk[:, :, r1 - r0:].transpose(1, 2)
     return out
 
 
@@ -70,37 +68,48 @@ def _block_rows(n: int, m0: int, m1: int, device) -> torch.Tensor:
     return idx
 
 
-def molecule_weights(c: torch.Tensor, dens: torch.Tensor, rho: torch.Tensor, u: torch.Tensor,
-                     w: torch.Tensor, upper: bool, abar: torch.Tensor | None = None,
-                     mbar: torch.Tensor | None = None):
-    """Packed Abar (N(N+1)/2, X) and Mbar (X, X) of one molecule.
+def chunk_weights(c: torch.Tensor, dens: torch.Tensor, rho: torch.Tensor, u: torch.Tensor,
+                  w: torch.Tensor, upper: bool, abar: torch.Tensor | None = None,
+                  mbar: torch.Tensor | None = None):
+    """Packed Abar (b, N(N+1)/2, X) and Mbar (b, X, X) for b molecules at once.
 
-    c (N, o) occupied factor (D = 2 c c^T), rho (X) whitened fitted density,
-    u (N, o, X) = B C (whitened), w (X, X) whitening factor (upper triangular
-    when ``upper``).  Abar rows are the packed pairs mu >= nu in row-major
-    order; each block of AO rows mu is one GEMM over nu < m1 followed by the
-    rank-one D (x) c term, so the full N*N*X tensor is never formed.
+    c (b, N, o) occupied factors (D = 2 c c^T), rho (b, X) whitened fitted
+    densities, u (b, N, o, X) = B C (whitened), w (b, X, X) whitening factors
+    (upper triangular when ``upper``).  Abar rows are the packed pairs
+    mu >= nu in row-major order; each block of AO rows mu is one batched GEMM
+    over nu < m1 followed by the rank-one D (x) c term, so the full N*N*X
+    tensor is never formed.  Every product is a batched GEMM over the b
+    molecules (a handful of launches per chunk instead of per molecule).
     """
-    n, o, x = u.shape
-    cvec = w @ rho  # raw-basis fitting coefficients c = Minv rho
-    bij = torch.einsum("mi,mjq->qij", c, u).reshape(x, o * o)  # C^T B_Q C
-    gam = _upper_times(w, bij) if upper else w @ bij  # Gamma[P, ij]
+    b, n, o, x = u.shape
+    cvec = torch.bmm(w, rho[:, :, None])[:, :, 0]  # raw-basis fitting coefficients Minv rho
+    # C^T B_Q C: [i][j][Q] from one GEMM, then [Q][i][j]
+    bij = torch.bmm(c.transpose(1, 2), u.reshape(b, n, o * x)).view(b, o, o, x)
+    bij = bij.permute(0, 3, 1, 2).reshape(b, x, o * o)
+    gam = _upper_times(w, bij) if upper else torch.bmm(w, bij)  # Gamma[P, ij]
     del bij
     # T[i][nu][P] = sum_j C[nu, j] Gamma[P, i, j]
-    t1 = torch.einsum("nj,pij->inp", c, gam.view(x, o, o)).reshape(o, n * x)
+    t = torch.bmm(gam.view(b, x * o, o), c.transpose(1, 2))  # [P][i][nu]
+    t1 = t.view(b, x, o, n).permute(0, 2, 3, 1).reshape(b, o, n * x)
+    del t
     if abar is None:
-        abar = torch.empty(n * (n + 1) // 2, x, dtype=u.dtype, device=u.device)
+        abar = torch.empty(b, n * (n + 1) // 2, x, dtype=u.dtype, device=u.device)
+    if mbar is None:
+        mbar = torch.empty(b, x, x, dtype=u.dtype, device=u.device)
     mu_all, nu_all = torch.tril_indices(n, n, device=u.device)
-    dpairs = dens[mu_all, nu_all]
+    dpairs = dens[:, mu_all, nu_all]
     for m0 in range(0, n, WEIGHT_ROW_BLOCK):
         m1 = min(n, m0 + WEIGHT_ROW_BLOCK)
-        blk = (c[m0:m1] @ t1[:, : m1 * x]).view(-1, x)  # (rows mu) x (nu < m1, P)
+        blk = torch.bmm(c[:, m0:m1], t1[:, :, : m1 * x]).view(b, -1, x)  # (mu) x (nu < m1, P)
         p0, p1 = m0 * (m0 + 1) // 2, m1 * (m1 + 1) // 2
-        torch.addr(blk[_block_rows(n, m0, m1, u.device)], dpairs[p0:p1], cvec, beta=-2.0,
-                   alpha=1.0, out=abar[p0:p1])
-    mbar = _sym_gram(gam, mbar)
-    mbar.addr_(cvec, cvec, alpha=-0.5)
+        abar[:, p0:p1] = torch.baddbmm(blk[:, _block_rows(n, m0, m1, u.device)],
+                                       dpairs[:, p0:p1, None], cvec[:, None, :], beta=-2.0, alpha=1.0)
+    _sym_gram(gam, mbar)
+    mbar.baddbmm_(cvec[:, :, None], cvec[:, None, :], alpha=-0.5)
     return abar, mbar
+
+
+WEIGHT_GROUP_BYTES = 4 << 30  # molecules per batched weight group: ~4 GB of (o, N, X) temporaries
 
 
 def df_rhf_gradient(chunk, ints, scf_out: dict, xyz: torch.Tensor) -> torch.Tensor:
@@ -127,8 +136,11 @@ def df_rhf_gradient(chunk, ints, scf_out: dict, xyz: torch.Tensor) -> torch.Tens
     abar = torch.empty(nb, n * (n + 1) // 2, x, dtype=torch.float64, device=dev)
     mbar = torch.empty(nb, x, x, dtype=torch.float64, device=dev)
     tri = mf.kind == "cholesky"
-    for m in range(nb):  # per molecule: bounded temporaries
-        molecule_weights(c[m], dens[m], rho_all[m], u_all[m], mf.inv_sqrt[m], tri, abar[m], mbar[m])
+    grp = max(1, WEIGHT_GROUP_BYTES // max(1, 8 * n * o * x))
+    for g0 in range(0, nb, grp):  # groups of molecules: bounded temporaries
+        g1 = min(nb, g0 + grp)
+        chunk_weights(c[g0:g1], dens[g0:g1], rho_all[g0:g1], u_all[g0:g1], mf.inv_sqrt[g0:g1], tri,
+                      abar[g0:g1], mbar[g0:g1])
     wctx.__exit__(None, None, None)
     grad = torch.zeros(plan.natom * 3, dtype=torch.float64, device=dev)
     st = torch.cuda.current_stream().cuda_stream
