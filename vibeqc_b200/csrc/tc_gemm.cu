@@ -198,10 +198,19 @@ __device__ __forceinline__ bool aborted(Ctrl* c) {
 // warps: 0 TMA producer, 1-8 splitters, 9 MMA issuer, 10-17 epilogue (two per
 // TMEM lane quarter, interleaved 16-column chunks): the split and the
 // TMEM -> HBM epilogue are per-warp latency-bound, so each has eight warps
-constexpr int kHalfThreads = 576;
-constexpr int kSplitWarps = 8;
+#ifndef VQC_HALF_SPLIT_WARPS
+#define VQC_HALF_SPLIT_WARPS 8
+#endif
+#ifndef VQC_HALF_EPI_WARPS
+#define VQC_HALF_EPI_WARPS 8
+#endif
+constexpr int kSplitWarps = VQC_HALF_SPLIT_WARPS;
+constexpr int kEpiWarps = VQC_HALF_EPI_WARPS;  // a multiple of 4 (TMEM lane quarters)
+constexpr int kEpiGroups = kEpiWarps / 4;      // warps sharing one lane quarter
 constexpr int kMmaWarp = 1 + kSplitWarps;
 constexpr int kEpiWarp0 = kMmaWarp + 1;
+constexpr int kHalfThreads = 32 * (kEpiWarp0 + kEpiWarps);
+static_assert(kEpiWarps % 4 == 0 && kEpiWarps >= 4, "epilogue warps per lane quarter");
 constexpr int kGramThreads = 320;
 constexpr int kTmemBuf = 128;  // columns per accumulator buffer (two buffers)
 
@@ -247,7 +256,7 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(af0 + 8 * b, 1);
-      mbar_init(ae0 + 8 * b, 8);
+      mbar_init(ae0 + 8 * b, kEpiWarps);
     }
     ctrl->abort = 0;
     ctrl->issued = ctrl->consumed = ctrl->commits = 0;
@@ -358,7 +367,7 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
         mma_commit(af0 + 8 * b);
       }
     }
-  } else {  // epilogue warps kEpiWarp0 .. kEpiWarp0 + 7
+  } else {  // epilogue warps kEpiWarp0 .. kEpiWarp0 + kEpiWarps - 1
     const int q = warp & 3;  // TMEM lane quarter this warp may access
     const int half = (warp - kEpiWarp0) >> 2;  // which interleaved 16-column chunks
     int t = 0;
@@ -391,7 +400,7 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
       float* ul = p.u_lo + (size_t)z * p.nocc * p.ldq + row;
       const double* cv = p.cvec + (size_t)z * p.nocc;
 #pragma unroll
-      for (int c = 16 * half; c < BN; c += 32) {
+      for (int c = 16 * half; c < BN; c += 16 * kEpiGroups) {
         float v[16];
         tmem_ld16(tmem + b * kTmemBuf + ((uint32_t)(q * 32) << 16) + c, v);
         if (valid) {
