@@ -35,7 +35,7 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "DF-RHF energy+force mol/s, K TFLOP/s; mixed vs FP64 GPU at |ΔE|≤1e-6 Eh"
 BASIS, AUX = "def2-svp", "cc-pvdz-jkfit"
-CPU_SAMPLE_SIZES = (2, 3, 4)
+CPU_SAMPLE_SIZES = (2, 3, 4, 5)
 # DRAM bytes (read + write) per algorithmic byte of the half transform,
 # measured by ncu on a (H2O)12 x 8 chunk: 3.697 GB read + 1.511 GB written
 # against 3.695 GB of FP32 B and 1.539 GB of split U
