@@ -292,6 +292,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         "clocks": clocks.summary(),
         "roofline": rl,
         "stages_ms_per_step": {k: round(v["ms"] / steps, 3) for k, v in stages.items()},
+        "scf_post_blocks": dict(__import__("vibeqc_b200.scf", fromlist=["POST_STATS"]).POST_STATS),
         "allocator": {"alloc_retries": int(torch.cuda.memory_stats().get("num_alloc_retries", 0)),
                       "peak_reserved_gb": round(torch.cuda.max_memory_reserved() / 2**30, 2)},
     }

@@ -85,3 +85,56 @@ def test_gradient_weights_match_dense_formulas(n, o, x, upper, monkeypatch):
         ref_mbar = -0.5 * torch.outer(cvec, cvec) + gam.reshape(x, -1) @ gam.reshape(x, -1).T
         assert torch.allclose(abar[m], ref_abar, rtol=0, atol=1e-11 * ref_abar.abs().max().item())
         assert torch.allclose(mbar[m], ref_mbar, rtol=0, atol=1e-11 * ref_mbar.abs().max().item())
+
+
+def _reference_diis(errs, focks):
+    """Pulay extrapolation over the given vectors (plain restatement)."""
+    nh = len(errs)
+    e = torch.stack(errs, dim=1)
+    f = torch.stack(focks, dim=1)
+    gram = torch.einsum("bimn,bjmn->bij", e, e)
+    nb = e.shape[0]
+    bmat = -torch.ones(nb, nh + 1, nh + 1, dtype=e.dtype)
+    bmat[:, nh, nh] = 0.0
+    bmat[:, :nh, :nh] = gram
+    rhs = torch.zeros(nb, nh + 1, 1, dtype=e.dtype)
+    rhs[:, nh, 0] = -1.0
+    w = torch.linalg.solve(bmat, rhs)[:, :nh, 0]
+    return torch.einsum("bh,bhmn->bmn", w, f)
+
+
+@pytest.mark.parametrize("with_rho", [False, True])
+def test_scf_post_ring_diis_matches_list_diis(with_rho):
+    g = torch.Generator().manual_seed(7)
+    nb, n, x, hist = 3, 9, 5, 4
+
+    def sym(*shape):
+        a = torch.randn(*shape, dtype=torch.float64, generator=g)
+        return a + a.transpose(-1, -2)
+
+    h, s_ = sym(nb, n, n), sym(nb, n, n) + 20 * torch.eye(n, dtype=torch.float64)
+    xo = torch.randn(nb, n, n, dtype=torch.float64, generator=g)
+    enuc = torch.randn(nb, dtype=torch.float64, generator=g)
+    post = scf._SCFPost(nb, n, x, hist, with_rho, "cpu")
+    post.load(h, s_, xo, enuc)
+    errs, focks = [], []
+    for it in range(7):  # wraps the ring
+        j, k, d = sym(nb, n, n), sym(nb, n, n), sym(nb, n, n)
+        rho = torch.randn(nb, x, dtype=torch.float64, generator=g)
+        f, energy, cmax, f_ext = post.run(j, k, d, rho if with_rho else None)
+        f_ref = h + j - 0.5 * k
+        fds = f_ref @ d @ s_
+        comm = fds - fds.transpose(1, 2)
+        errs.append(xo.transpose(1, 2) @ comm @ xo)
+        focks.append(f_ref)
+        errs, focks = errs[-hist:], focks[-hist:]
+        ext_ref = _reference_diis(errs, focks) if len(errs) > 1 else f_ref
+        if with_rho:
+            e_ref = (torch.einsum("bmn,bmn->b", d, h) + 0.5 * (rho * rho).sum(1)
+                     - 0.25 * torch.einsum("bmn,bmn->b", d, k) + enuc)
+        else:
+            e_ref = 0.5 * torch.einsum("bmn,bmn->b", d, h + f_ref) + enuc
+        assert torch.allclose(f, f_ref, atol=1e-12)
+        assert torch.allclose(energy, e_ref, atol=1e-10)
+        assert torch.allclose(cmax, comm.abs().amax(dim=(1, 2)), atol=1e-10)
+        assert torch.allclose(f_ext, ext_ref, rtol=1e-8, atol=1e-8)

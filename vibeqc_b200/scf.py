@@ -345,23 +345,136 @@ def whiten_in_place(a: torch.Tensor, mf: MetricFactor) -> None:
             rows[:, :, c0:c1].copy_(torch.matmul(rows[:, :, :c1], w[:, :c1, c0:c1]))
 
 
-def _diis_extrapolate(errs: list, focks: list) -> torch.Tensor:
-    nh = len(errs)
-    e = torch.stack(errs, dim=1)  # (nb, h, N, N)
-    f = torch.stack(focks, dim=1)
-    nb = e.shape[0]
-    gram = torch.einsum("bimn,bjmn->bij", e, e)
-    bmat = -torch.ones(nb, nh + 1, nh + 1, dtype=e.dtype, device=e.device)
-    bmat[:, nh, nh] = 0.0
-    bmat[:, :nh, :nh] = gram
-    rhs = torch.zeros(nb, nh + 1, 1, dtype=e.dtype, device=e.device)
-    rhs[:, nh, 0] = -1.0
-    # scale rows for conditioning; fall back to the latest Fock on failure
-    w, info = torch.linalg.solve_ex(bmat, rhs)
-    w = w[:, :nh, 0]
-    ok = (info == 0) & torch.isfinite(w).all(dim=1)
-    ext = torch.einsum("bh,bhmn->bmn", w, f)
-    return torch.where(ok[:, None, None], ext, focks[-1])
+def _graphs_enabled() -> bool:
+    return (os.environ.get("VQC_CUDA_GRAPHS", "1") != "0"
+            and os.environ.get("VQC_SP2_GRAPHS", "1") != "0")
+
+
+class _SCFPost:
+    """Fock, energy, commutator and DIIS extrapolation of one SCF iteration.
+
+    Everything between a J/K build and the density update runs on static
+    buffers and, when CUDA graphs are enabled, as one captured graph: the
+    per-iteration work is ~25 small kernels whose host dispatch cost more
+    than their GPU time.  DIIS keeps its error and Fock vectors in a ring of
+    ``hist`` slots with an incrementally updated Gram matrix; slots not yet
+    filled get identity rows in the Pulay system, so their weights are
+    exactly zero and the extrapolation equals the usual one over the last
+    ``min(count, hist)`` iterations (the order of the vectors does not
+    matter).  ``with_rho`` selects the energy formula of the anchored phase,
+    E = tr(DH) + |rho|^2/2 - tr(DK)/4 + E_nn, instead of tr(D(H+F))/2 + E_nn.
+    """
+
+    def __init__(self, nb: int, n: int, x: int, hist: int, with_rho: bool, device):
+        f64 = dict(dtype=torch.float64, device=device)
+        self.h, self.s, self.xo = (torch.zeros(nb, n, n, **f64) for _ in range(3))
+        self.enuc = torch.zeros(nb, **f64)
+        self.j, self.k, self.d = (torch.zeros(nb, n, n, **f64) for _ in range(3))
+        self.rho = torch.zeros(nb, x, **f64)
+        self.e_ring = torch.zeros(nb, hist, n, n, **f64)
+        self.f_ring = torch.zeros(nb, hist, n, n, **f64)
+        self.gram = torch.zeros(nb, hist, hist, **f64)
+        self.count = torch.zeros(1, dtype=torch.int64, device=device)
+        self.hist, self.with_rho = hist, with_rho
+        self.eye = torch.eye(hist, **f64)
+        self.out = None
+        self.graph = None
+        if _graphs_enabled() and torch.device(device).type == "cuda":
+            try:
+                side = torch.cuda.Stream(device=device)
+                side.wait_stream(torch.cuda.current_stream(device))
+                with torch.cuda.stream(side):  # warm-up outside capture
+                    self._step()
+                torch.cuda.current_stream(device).wait_stream(side)
+                self.reset()
+                graph = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(graph):
+                    self.out = self._step()
+                self.graph = graph
+            except Exception:  # a capture the runtime refuses: run the same ops eagerly
+                torch.cuda.synchronize(device)
+                self.graph = None
+        self.reset()
+
+    def reset(self) -> None:
+        self.count.zero_()
+        self.gram.zero_()
+
+    def load(self, h, s, xo, enuc) -> None:
+        self.h.copy_(h)
+        self.s.copy_(s)
+        self.xo.copy_(xo)
+        self.enuc.copy_(enuc)
+        # empty slots carry weight 0; zeros keep a previous chunk's values out
+        self.e_ring.zero_()
+        self.f_ring.zero_()
+        self.reset()
+
+    def _step(self):
+        hist = self.hist
+        f = self.h + self.j - 0.5 * self.k
+        if self.with_rho:
+            energy = (torch.einsum("bmn,bmn->b", self.d, self.h)
+                      + 0.5 * (self.rho * self.rho).sum(dim=1)
+                      - 0.25 * torch.einsum("bmn,bmn->b", self.d, self.k) + self.enuc)
+        else:
+            energy = 0.5 * torch.einsum("bmn,bmn->b", self.d, self.h + f) + self.enuc
+        fds = f @ self.d @ self.s
+        comm = fds - fds.transpose(1, 2)
+        cmax = comm.abs().amax(dim=(1, 2))
+        err = self.xo.transpose(1, 2) @ comm @ self.xo
+        slot = torch.remainder(self.count, hist)
+        self.e_ring.index_copy_(1, slot, err[:, None])
+        self.f_ring.index_copy_(1, slot, f[:, None])
+        g_new = torch.einsum("bmn,bhmn->bh", err, self.e_ring)
+        self.gram.index_copy_(1, slot, g_new[:, None, :])
+        self.gram.index_copy_(2, slot, g_new[:, :, None])
+        self.count.add_(1)
+        valid = torch.arange(hist, device=self.count.device) < torch.clamp(self.count, max=hist)
+        vf = valid.to(torch.float64)
+        pair = vf[:, None] * vf[None, :]
+        nb = f.shape[0]
+        bmat = torch.zeros(nb, hist + 1, hist + 1, dtype=torch.float64, device=f.device)
+        bmat[:, :hist, :hist] = self.gram * pair + self.eye * (1.0 - vf)[None, :, None]
+        bmat[:, hist, :hist] = -vf
+        bmat[:, :hist, hist] = -vf
+        rhs = torch.zeros(nb, hist + 1, 1, dtype=torch.float64, device=f.device)
+        rhs[:, hist, 0] = -1.0
+        w, info = torch.linalg.solve_ex(bmat, rhs)
+        w = w[:, :hist, 0] * vf
+        ok = (info == 0) & torch.isfinite(w).all(dim=1)
+        ext = torch.einsum("bh,bhmn->bmn", w, self.f_ring)
+        f_ext = torch.where(ok[:, None, None], ext, f)
+        return f, energy, cmax, f_ext
+
+    def run(self, j, k, d, rho=None):
+        """(F, energy, max|FDS - SDF|, extrapolated F); outputs are overwritten next call."""
+        self.j.copy_(j)
+        self.k.copy_(k)
+        self.d.copy_(d)
+        if rho is not None:
+            self.rho.copy_(rho)
+        if self.graph is not None:
+            self.graph.replay()
+            return self.out
+        return self._step()
+
+
+_POST: dict = {}
+POST_CACHE_BYTES = 4 << 30
+POST_STATS = {"graphs": 0, "eager": 0}  # how the cached post-build blocks run
+
+
+def _scf_post(nb, n, x, hist, with_rho, device) -> _SCFPost:
+    key = (nb, n, x, hist, with_rho, str(device))
+    p = _POST.get(key)
+    if p is None:
+        held = sum(2 * v.e_ring.numel() * 8 for v in _POST.values())
+        if held + 2 * nb * hist * n * n * 8 > POST_CACHE_BYTES:
+            _POST.clear()
+        p = _POST[key] = _SCFPost(nb, n, x, hist, with_rho, device)
+        POST_STATS["graphs" if p.graph is not None else "eager"] += 1
+    return p
 
 
 def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision: str = "fp64",
@@ -418,7 +531,7 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
     d_final = d.clone()
     c_final = c.clone()
     f_final = torch.zeros_like(d)
-    errs, focks = [], []
+    post = None
     comm_tol = 10.0 * min(1e-8, density_tolerance)
     # mixed precision runs two phases per chunk:
     #   "tc":     plain tensor-core J/K until max|FDS-SDF| <= ANCHOR_COMMUTATOR
@@ -452,20 +565,21 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
         phase_iterations += 1
         TIMER_ctx = TIMER.stage("scf_other")
         TIMER_ctx.__enter__()
-        f = h + j - 0.5 * k
-        if rho is not None:
-            # E = tr(D H) + |rho|^2 / 2 - tr(D K) / 4 + E_nn from the FP64-accurate rho, K
-            energy = (torch.einsum("bmn,bmn->b", d, h) + 0.5 * (rho * rho).sum(dim=1)
-                      - 0.25 * torch.einsum("bmn,bmn->b", d, k) + enuc)
-        else:
-            energy = 0.5 * torch.einsum("bmn,bmn->b", d, h + f) + enuc
-        fds = f @ d @ s
-        comm = fds - fds.transpose(1, 2)
-        err = xo.transpose(1, 2) @ comm @ xo
-        errs.append(err)
-        focks.append(f)
-        errs, focks = errs[-diis_history:], focks[-diis_history:]
-        f_ext = _diis_extrapolate(errs, focks) if len(errs) > 1 else f
+        # Fock, energy, commutator, DIIS: one captured graph per (shape, formula);
+        # the anchored phase (E from the FP64-accurate rho and K) has its own,
+        # which continues the DIIS history of the tensor-core phase
+        with_rho = rho is not None
+        if post is None or post.with_rho != with_rho:
+            prev = post
+            post = _scf_post(nb, n, x, diis_history, with_rho, dev)
+            post.load(h, s, xo, enuc)
+            if prev is not None and not ANCHOR_DIIS_RESET:
+                post.e_ring.copy_(prev.e_ring)
+                post.f_ring.copy_(prev.f_ring)
+                post.gram.copy_(prev.gram)
+                post.count.copy_(prev.count)
+        f, energy, cmax, f_ext = post.run(j, k, d, rho)
+        energy = energy.clone()
         TIMER_ctx.__exit__(None, None, None)
         # the tensor-core phase only needs the projector to its own accuracy
         if phase == "anchor":
@@ -480,14 +594,11 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
         de = (energy - e_old).abs()
         de = torch.where(torch.isnan(de), torch.full_like(de, float("inf")), de)
         drms = ((d_new - d) ** 2).mean(dim=(1, 2)).sqrt()
-        cmax = comm.abs().amax(dim=(1, 2))
         done = (de < energy_tolerance) & (drms < density_tolerance) & (cmax <= comm_tol)
         if phase == "tc":
             loose = cmax <= ANCHOR_COMMUTATOR
             if bool((loose | ~active).all()) or phase_iterations >= MIXED_ITERATION_CAP:
                 phase, phase_iterations = "anchor", 0
-                if ANCHOR_DIIS_RESET:
-                    errs, focks = [], []
             done = torch.zeros_like(done)
         if trace is not None:
             trace.append((it, phase, float(de[active].max()) if bool(active.any()) else 0.0,
