@@ -292,7 +292,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         "clocks": clocks.summary(),
         "roofline": rl,
         "stages_ms_per_step": {k: round(v["ms"] / steps, 3) for k, v in stages.items()},
-        "scf_post_blocks": dict(__import__("vibeqc_b200.scf", fromlist=["POST_STATS"]).POST_STATS),
+        "scf_graphs": scf_graph_stats(),
         "allocator": {"alloc_retries": int(torch.cuda.memory_stats().get("num_alloc_retries", 0)),
                       "peak_reserved_gb": round(torch.cuda.max_memory_reserved() / 2**30, 2)},
     }
@@ -307,6 +307,16 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         out["k_tflops"] = round(model["k_flops_per_build"] * builds / t_k / 1e12, 2)
     batch.close()
     return out
+
+
+def scf_graph_stats() -> dict:
+    """How the cached SCF blocks run: captured CUDA graphs or eager launches."""
+    from vibeqc_b200 import scf as scfmod
+
+    occ = [g.graph is not None for g in scfmod._OCC.values()]
+    return {"post_block_graphs": scfmod.POST_STATS["graphs"],
+            "post_block_eager": scfmod.POST_STATS["eager"],
+            "occupied_factor_graphs": sum(occ), "occupied_factor_eager": len(occ) - sum(occ)}
 
 
 def _peaks() -> dict:

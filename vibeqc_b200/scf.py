@@ -287,6 +287,65 @@ def purify_sp2(fo: torch.Tensor, nocc: int, max_steps: int = 96, tol: float = 1e
     return 0.5 * (g.x + g.x.transpose(1, 2))
 
 
+def _cholqr2(y: torch.Tensor):
+    """Two Cholesky-QR passes (orthonormal columns); ok[b] False where a Gram factor failed."""
+    ok = torch.ones(y.shape[0], dtype=torch.bool, device=y.device)
+    eye = torch.eye(y.shape[-1], dtype=y.dtype, device=y.device)
+    for _ in range(2):
+        g = torch.bmm(y.transpose(1, 2), y)
+        u, info = torch.linalg.cholesky_ex(g, upper=True)
+        ok &= info == 0
+        u = torch.where((info == 0)[:, None, None], u, eye)
+        y = torch.linalg.solve_triangular(u, y, upper=True, left=False)
+    return y, ok
+
+
+class _OccGraph:
+    """proj @ (guess + scale * noise) made orthonormal, as one CUDA graph per shape."""
+
+    def __init__(self, nb: int, n: int, o: int, scale: float, device):
+        f64 = dict(dtype=torch.float64, device=device)
+        self.proj = torch.zeros(nb, n, n, **f64)
+        self.guess = torch.zeros(nb, n, o, **f64)
+        self.noise = torch.zeros(nb, n, o, **f64)
+        self.scale = scale
+        self.out = None
+        self.graph = None
+        self.guess[:, :o, :] = torch.eye(o, **f64)[None]  # well-posed warm-up input
+        self.proj[:, :, :] = torch.eye(n, **f64)[None]
+        if _graphs_enabled() and torch.device(device).type == "cuda":
+            try:
+                side = torch.cuda.Stream(device=device)
+                side.wait_stream(torch.cuda.current_stream(device))
+                with torch.cuda.stream(side):
+                    self._step()
+                torch.cuda.current_stream(device).wait_stream(side)
+                graph = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(graph):
+                    self.out = self._step()
+                self.graph = graph
+            except Exception:  # a capture the runtime refuses: run the same ops eagerly
+                torch.cuda.synchronize(device)
+                self.graph = None
+
+    def _step(self):
+        return _cholqr2(torch.bmm(self.proj, self.guess + self.scale * self.noise))
+
+    def run(self, proj, guess, gen):
+        self.proj.copy_(proj)
+        self.guess.copy_(guess)
+        torch.randn(self.noise.shape, dtype=self.noise.dtype, device=self.noise.device,
+                    generator=gen, out=self.noise)
+        if self.graph is not None:
+            self.graph.replay()
+            y, ok = self.out
+            return y.clone(), ok
+        return self._step()
+
+
+_OCC: dict = {}
+
+
 def occupied_factor(proj: torch.Tensor, guess: torch.Tensor, gen: torch.Generator,
                     noise_scale: float = 0.3) -> torch.Tensor:
     """Orthonormal basis of range(proj) by Cholesky-QR2 of proj @ (guess + noise).
@@ -296,22 +355,24 @@ def occupied_factor(proj: torch.Tensor, guess: torch.Tensor, gen: torch.Generato
     a molecule whose factorisation still fails is retried with a purely random
     start.  With ``noise_scale=0`` the result is the projected guess made
     orthonormal, so it stays within O(|proj - guess guess^T|) of ``guess``.
+    The first attempt runs as a cached CUDA graph per (shape, noise scale).
     """
-    noise = torch.randn(guess.shape, dtype=guess.dtype, device=guess.device, generator=gen)
-    start = guess + noise_scale * noise
-    for attempt in range(2):
-        y = torch.bmm(proj, start)
-        ok = torch.ones(y.shape[0], dtype=torch.bool, device=y.device)
-        for _ in range(2):
-            g = torch.bmm(y.transpose(1, 2), y)
-            u, info = torch.linalg.cholesky_ex(g, upper=True)
-            ok &= info == 0
-            eye = torch.eye(g.shape[-1], dtype=g.dtype, device=g.device)
-            u = torch.where((info == 0)[:, None, None], u, eye)
-            y = torch.linalg.solve_triangular(u, y, upper=True, left=False)
-        if bool(ok.all()):
-            return y
-        start = torch.where(ok[:, None, None], start, noise)
+    nb, n, o = guess.shape
+    key = (nb, n, o, float(noise_scale), str(guess.device))
+    og = _OCC.get(key)
+    if og is None:
+        if len(_OCC) > 64:
+            _OCC.clear()
+        og = _OCC[key] = _OccGraph(nb, n, o, float(noise_scale), guess.device)
+    y, ok = og.run(proj, guess, gen)
+    if bool(ok.all()):
+        return y
+    # retry the failed molecules from a purely random start
+    noise = og.noise.clone()
+    start = torch.where(ok[:, None, None], guess + noise_scale * noise, noise)
+    y, ok = _cholqr2(torch.bmm(proj, start))
+    if bool(ok.all()):
+        return y
     raise FloatingPointError("occupied-space factorisation failed")
 
 
