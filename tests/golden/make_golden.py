@@ -31,7 +31,7 @@ from vibeqc_b200 import geometry  # noqa: E402
 
 OUT = HERE / "df_rhf_golden.json"
 
-# the survey smoke geometry (Bohr): a water with a symmetric frame
+# a single-water smoke geometry (Bohr) with a symmetric frame
 WATER_SMOKE = [("O", (0.0, 0.0, 0.0)), ("H", (0.0, 1.432, 1.107)), ("H", (0.0, -1.432, 1.107))]
 
 

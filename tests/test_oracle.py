@@ -38,7 +38,7 @@ def test_oracle_matches_reference_golden(name):
     assert np.abs(res.forces - np.array(case["forces"])).max() < 5e-8
 
 
-def test_golden_survey_energy_pin():
+def test_golden_water_smoke_energy_pin():
     # the water/def2-SVP smoke number recorded from the reference
     assert GOLDEN["h2o_def2svp_auxdef2svp"]["energy"] == pytest.approx(-76.17929112830237, abs=1e-10)
 
