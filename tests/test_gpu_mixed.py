@@ -62,3 +62,16 @@ def test_decane_mixed_matches_fp64():
     assert c64 and cmx
     assert abs(emx - e64) <= 1e-6
     assert np.abs(fmx - f64).max() <= 1e-5
+
+
+def test_mixed_request_beyond_kernel_limits_runs_fp64():
+    """(H2O)22 in def2-SVP has N = 528 > 512: its chunk runs the FP64 GPU path."""
+    from vibeqc_b200 import Calculator, geometry
+
+    calc = Calculator(method="rhf", basis="def2-svp", auxiliary_basis="cc-pvdz-jkfit", device="cuda",
+                      density_fitting="cuda", precision="mixed")
+    batch = calc.prepare_batch([geometry.water_cluster(22, 0), geometry.water_cluster(3, 0)])
+    res = batch.execute(properties=("energy",))
+    assert res.items[0].succeeded and res.items[0].precision == {"mode": "fp64", "requested": "mixed"}
+    assert res.items[1].succeeded and res.items[1].precision == {"mode": "mixed", "requested": "mixed"}
+    batch.close()

@@ -138,3 +138,13 @@ def test_scf_post_ring_diis_matches_list_diis(with_rho):
         assert torch.allclose(energy, e_ref, atol=1e-10)
         assert torch.allclose(cmax, comm.abs().amax(dim=(1, 2)), atol=1e-10)
         assert torch.allclose(f_ext, ext_ref, rtol=1e-8, atol=1e-8)
+
+
+def test_chunk_precision_respects_mixed_kernel_limits():
+    from vibeqc_b200.calculator import chunk_precision
+
+    assert chunk_precision("mixed", 384, 80) == "mixed"
+    assert chunk_precision("mixed", 512, 128) == "mixed"
+    assert chunk_precision("mixed", 513, 80) == "fp64"   # FP32 B rows beyond 512
+    assert chunk_precision("mixed", 400, 129) == "fp64"  # MMA N beyond 128
+    assert chunk_precision("fp64", 100, 10) == "fp64"

@@ -205,13 +205,15 @@ class PreparedBatch:
         if budget <= 0:
             budget = int(0.6 * torch.cuda.get_device_properties(calculator.device).total_memory)
         self._chunks = []
-        for (nao, naux, _), idx in sorted(groups.items()):
-            per_mol = _device_bytes_per_molecule(nao, naux, calculator.precision)
+        for (nao, naux, nocc), idx in sorted(groups.items()):
+            prec = chunk_precision(calculator.precision, nao, nocc)
+            per_mol = _device_bytes_per_molecule(nao, naux, prec)
             limit = max(1, budget // per_mol)
             for s in range(0, len(idx), limit):
                 part = idx[s:s + limit]
-                self._chunks.append(Chunk([self._molecules[i] for i in part], part,
-                                          calculator.spherical))
+                chunk = Chunk([self._molecules[i] for i in part], part, calculator.spherical)
+                chunk.precision = prec
+                self._chunks.append(chunk)
         self._natoms = [len(m.atomic_numbers) for m in self._molecules]
         self.atomic_numbers = tuple(tuple(int(z) for z in m.atomic_numbers) for m in self._molecules)
 
@@ -251,7 +253,7 @@ class PreparedBatch:
         """Integrals, SCF and (optionally) the gradient of one chunk, all on device."""
         calc = self._calc
         ints = compute_integrals(chunk.plan, xyz)
-        out = run_scf(chunk, ints, xyz, precision=calc.precision,
+        out = run_scf(chunk, ints, xyz, precision=chunk.precision,
                       max_iterations=calc.max_iterations,
                       energy_tolerance=calc.energy_tolerance,
                       density_tolerance=calc.density_tolerance,
@@ -380,12 +382,31 @@ class PreparedBatch:
                                         "metric_rank": int(out["metric_rank"][j]),
                                         "metric_condition": float(out["metric_condition"][j]),
                                         "metric_factor": out["metric_kind"]},
-                        precision={"mode": calc.precision},
+                        precision={"mode": chunk.precision, "requested": calc.precision},
                     )
         result = BatchResult(tuple(items))
         if strict:
             result.raise_for_failures()
         return result
+
+
+# limits of the mixed-precision kernels: MMA N = round_up(n_occ, 16) <= 128 and
+# FP32 B rows round_up(N, 4) <= 512 (Coulomb / fitted-density accumulators)
+MIXED_MAX_NOCC = 128
+MIXED_MAX_NAO = 512
+
+
+def chunk_precision(requested: str, nao: int, nocc: int) -> str:
+    """Precision a chunk runs in: "mixed" only inside the mixed kernels' limits.
+
+    Molecules beyond them (more than 128 occupied orbitals or 512 basis
+    functions) run the FP64 GPU path; each item's ``precision`` record says so.
+    """
+    if requested != "mixed":
+        return requested
+    if (nocc + 15) // 16 * 16 > MIXED_MAX_NOCC or (nao + 3) // 4 * 4 > MIXED_MAX_NAO:
+        return "fp64"
+    return "mixed"
 
 
 def _device_bytes_per_molecule(nao: int, naux: int, precision: str) -> int:

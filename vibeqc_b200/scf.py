@@ -179,6 +179,7 @@ class Chunk:
             if (l_.nao, l_.naux, l_.nocc) != (self.nao, self.naux, self.nocc):
                 raise ValueError("a chunk must be homogeneous in (N, X, n_occ)")
         self.natoms = [len(m.atomic_numbers) for m in molecules]
+        self.precision = "fp64"  # set by the prepared batch from the requested precision
 
     def close(self):
         self.plan.close()
