@@ -359,7 +359,10 @@ def df_rhf(atoms, basis="def2-svp", auxiliary_basis="cc-pvdz-jkfit", *, spherica
         drms = float(np.sqrt(np.mean((d_new - d) ** 2)))
         comm = float(np.abs(err).max())
         e_old = energy
-        if de < energy_tolerance and drms < density_tolerance and comm <= min(1e-8, density_tolerance) * 10:
+        # src/scf/cuda/scf_convergence_policy.cuh:28-37 (roundoff guard 16 eps,
+        # src/scf/cuda/scf_constants.hpp:16-17)
+        guard = 16.0 * 2.220446049250313e-16 * max(1.0, abs(energy), abs(e_old or 0.0))
+        if de < energy_tolerance + guard and drms < density_tolerance and comm <= min(1e-8, density_tolerance):
             converged = True
             break
         d = d_new

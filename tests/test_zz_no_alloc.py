@@ -5,8 +5,9 @@ memory is owned by another allocator's pool, or they must avoid the
 synchronisation cudaFree implies): its partial sums live in a fixed array
 inside the library.  Two calls in a row must both reproduce the workspace
 entry point, so nothing left in the shared array from a previous call leaks
-into a result.  The file name makes pytest collect it last, so it runs alone in
-a fresh process and after every other GPU test.
+into a result.  The file name makes pytest collect it last, in the same
+process as the other GPU tests and after them; it also passes when run on its
+own in a fresh process.
 """
 
 import pytest

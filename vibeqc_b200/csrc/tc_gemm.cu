@@ -728,13 +728,11 @@ template <int BN>
 static int launch_half(const CUtensorMap& ta, const CUtensorMap& th, const CUtensorMap& tl,
                        const HalfParams& p, cudaStream_t st) {
   using C = HalfCfg<BN>;
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(half_ws_kernel<BN>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
-    if (e != cudaSuccess) return cuda_status(e, "half smem attribute");
-    attr = true;
-  }
+  // the opt-in is a property of the current device's context: set it on every
+  // launch (cheap) so a process that drives several GPUs gets it on each
+  cudaError_t e = cudaFuncSetAttribute(half_ws_kernel<BN>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
+  if (e != cudaSuccess) return cuda_status(e, "half smem attribute");
   const int grid = (p.nitems + p.per_cta - 1) / p.per_cta;
   half_ws_kernel<BN><<<grid, kHalfThreads, C::SMEM, st>>>(ta, th, tl, p);
   count_launch();
@@ -842,13 +840,10 @@ static int launch_gram(const float* a_hi, const float* a_lo, const float* b_hi, 
   p.nseg = nseg;
   p.kout = kout;
   p.error = error;
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(gram_ws_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         GramCfg::SMEM);
-    if (e != cudaSuccess) return cuda_status(e, "gram smem attribute");
-    attr = true;
-  }
+  // per current device (see launch_half)
+  cudaError_t e = cudaFuncSetAttribute(gram_ws_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       GramCfg::SMEM);
+  if (e != cudaSuccess) return cuda_status(e, "gram smem attribute");
   dim3 grid(tiles, nmol * ksplit);
   gram_ws_kernel<<<grid, kGramThreads, GramCfg::SMEM, (cudaStream_t)stream>>>(ah, al, bh, bl, p);
   count_launch();

@@ -62,4 +62,6 @@ def main(root: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: python extract_basis.py <generativeqc source checkout>")
+    main(Path(sys.argv[1]))

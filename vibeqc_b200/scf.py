@@ -8,9 +8,10 @@ share one native plan and run their SCF iterations as batched device work
 SCF semantics follow ``src/scf/solver/mean_field_driver.cpp:233``: core-
 Hamiltonian guess, F = H + J - K/2, E = 1/2 tr D(H + F) + E_nn, Pulay DIIS on
 the orthogonalised commutator X^T (FDS - SDF) X with ``diis_history`` vectors,
-and convergence when |dE| < energy_tolerance, rms(dD) < density_tolerance and
-max|FDS - SDF| <= 10 * min(1e-8, density_tolerance)
-(``src/scf/cuda/scf_convergence_policy.cuh:28-37``).
+and convergence when |dE| < energy_tolerance + 16 eps max(1, |E|, |E_old|),
+rms(dD) < density_tolerance and max|FDS - SDF| <= min(1e-8, density_tolerance)
+(``src/scf/cuda/scf_convergence_policy.cuh:18-37``, constants
+``src/scf/cuda/scf_constants.hpp:16-17``).
 """
 
 from __future__ import annotations
@@ -146,6 +147,11 @@ def factor_metric(metric: torch.Tensor, relative_threshold: float = 1e-10) -> Me
     cond = (lmax[:, 0] / lmin).tolist()
     return MetricFactor(lam, vec, keep, inv_sqrt, rank, cond, "eigen")
 
+
+# energy-change roundoff allowance of the reference's stopping rule:
+# 16 * DBL_EPSILON * max(1, |E|, |E_old|)
+ENERGY_ROUNDOFF_FACTOR = 16.0
+DOUBLE_EPS = 2.220446049250313e-16
 
 MIXED_ITERATION_CAP = 40  # plain tensor-core iterations before the anchor is forced
 ANCHOR_COMMUTATOR = 1e-5  # max|FDS - SDF| at which the FP64 anchor is formed
@@ -594,7 +600,7 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
     c_final = c.clone()
     f_final = torch.zeros_like(d)
     post = None
-    comm_tol = 10.0 * min(1e-8, density_tolerance)
+    comm_tol = min(1e-8, density_tolerance)
     # mixed precision runs two phases per chunk:
     #   "tc":     plain tensor-core J/K until max|FDS-SDF| <= ANCHOR_COMMUTATOR
     #             for every active molecule (or MIXED_ITERATION_CAP).  Their
@@ -656,7 +662,9 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
         de = (energy - e_old).abs()
         de = torch.where(torch.isnan(de), torch.full_like(de, float("inf")), de)
         drms = ((d_new - d) ** 2).mean(dim=(1, 2)).sqrt()
-        done = (de < energy_tolerance) & (drms < density_tolerance) & (cmax <= comm_tol)
+        guard = ENERGY_ROUNDOFF_FACTOR * DOUBLE_EPS * torch.clamp(
+            torch.maximum(energy.abs(), e_old.abs().nan_to_num(0.0)), min=1.0)
+        done = (de < energy_tolerance + guard) & (drms < density_tolerance) & (cmax <= comm_tol)
         if phase == "tc":
             loose = cmax <= ANCHOR_COMMUTATOR
             if bool((loose | ~active).all()) or phase_iterations >= MIXED_ITERATION_CAP:
