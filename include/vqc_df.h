@@ -5,8 +5,9 @@
  * void*. No C++ or torch types cross this boundary.  Every entry point returns
  * a status in the reference's generativeqc_status vocabulary
  * (include/generativeqc/generativeqc.h:23-42 of the reference):
- *   0 success, 1 invalid argument, 4 not converged, 5 numerical failure,
- *   6 CUDA error, 7 out of memory.
+ *   0 success, 1 invalid argument, 2 ABI mismatch (a descriptor whose
+ *   struct_size/abi_version this library does not accept), 4 not converged,
+ *   5 numerical failure, 6 CUDA error, 7 out of memory.
  * A thread-local detail string is available from vqc_last_error() (same idea as
  * generativeqc_context_get_last_detail, generativeqc.h:1231).
  *
@@ -19,6 +20,7 @@
 #ifndef VQC_DF_H
 #define VQC_DF_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -30,6 +32,7 @@ extern "C" {
 enum {
   VQC_STATUS_SUCCESS = 0,
   VQC_STATUS_INVALID_ARGUMENT = 1,
+  VQC_STATUS_ABI_MISMATCH = 2,
   VQC_STATUS_NOT_CONVERGED = 4,
   VQC_STATUS_NUMERICAL_FAILURE = 5,
   VQC_STATUS_CUDA_ERROR = 6,
@@ -123,6 +126,67 @@ int vqc_grad3c(vqc_plan* plan, const double* xyz, const double* abar_packed, dou
 int vqc_grad2c(vqc_plan* plan, const double* xyz, const double* mbar, double* grad, void* stream);
 int vqc_grad1e(vqc_plan* plan, const double* xyz, const double* dens, const double* wdens,
                double* grad, void* stream);
+
+/*
+ * Standalone DF gradient contraction with the contract of the reference's
+ * generativeqc_system_df_gradient_cuda (include/generativeqc/generativeqc.h:
+ * 1312-1333; src/api/c_api_df_gradient.cpp:11):
+ *   gradient[a][x] = sum_{mu,nu,P} bar_a[mu][nu][P] d(mu nu|P)/dR_ax
+ *                  + sum_{P,Q} bar_m[P][Q] d(P|Q)/dR_ax
+ * system: exactly one molecule (its orbital and auxiliary shells); xyz: HOST
+ * [natom][3] Bohr.  bar_a: HOST full row-major [mu][nu][P], count_a = N*N*X;
+ * bar_m: HOST full row-major [P][Q], count_m = X*X; either may be NULL
+ * (that channel is zero; the counts must still match).  Nonsymmetric weights
+ * are allowed and every element is counted once.  gradient: HOST [natom][3],
+ * gradient_count = 3*natom, DF terms only; written only on success (failures
+ * leave it untouched).  maximum_bytes (> 0) bounds the device memory of the
+ * weights: bar_a is streamed in auxiliary-shell column tiles of at most
+ * maximum_tile_elements (0: automatic) elements of N*N*X_tile.
+ * schedule 0 or 1 (the reference's thread / serial traversal) selects the
+ * same kernels here; their floating-point atomics make the summation order,
+ * hence the last bits, vary between calls.  resources (optional; struct_size
+ * and abi_version must be set, else status 2) receives the staging record.
+ * Runs on the current device's default stream and synchronises before it
+ * returns.
+ */
+typedef struct {
+  uint32_t struct_size;
+  uint32_t abi_version;
+  uint64_t host_bytes, device_bytes, host_to_device_bytes, device_to_host_bytes;
+  uint64_t weight_tile_elements, tiles, uploads, stream_synchronizations;
+} vqc_df_gradient_resources;
+
+int vqc_df_gradient(const vqc_batch_desc* system, const double* xyz, const double* bar_a,
+                    size_t count_a, const double* bar_m, size_t count_m, uint32_t schedule,
+                    size_t maximum_bytes, size_t maximum_tile_elements, double* gradient,
+                    size_t gradient_count, vqc_df_gradient_resources* resources);
+
+/*
+ * FP64-accurate products on the int8 tensor cores (slices of 7 bits with exact
+ * int32 accumulation; tcgen05.mma kind::i8).  Used for the whitening
+ * B = A W of the mixed-precision path (reference src/scf/density_fitting.cpp:
+ * 711-764 and src/scf/cuda/df_plan_setup.cpp:34,70, an FP64 GEMM there).
+ *   vqc_ozaki_slice_rows: rows of src (nmol blocks of `rows` rows, row stride
+ *     ld, block stride mol_stride; each element times col_scale[mol][col]
+ *     when col_scale is not NULL -- exact powers of two) -> exps[mol][row]
+ *     (max |row| < 2^e) and nslices (1..7) int8 slices
+ *     dst[mol][slice][row][ldd] with row * 2^-e = sum_s dst_s 2^-7s + r,
+ *     |r| <= 2^-7 nslices.  Columns >= cols of dst are not written.
+ *   vqc_ozaki_gemm: c[mol][r][n] (row stride ldc, block stride c_mol_stride)
+ *     = sum_k A[mol][r][k] B[mol][n][k] from the slices of A (m rows) and B
+ *     (n rows), both [mol][slice][row][ldk] (ldk % 16 == 0, k <= ldk) with
+ *     their exponents, keeping slice pairs s + t <= nslices + 1.  upper != 0:
+ *     B[mol][n][k] = 0 for k > n (only those K are read).  k * nslices *
+ *     127^2 must stay below 2^31.  error: device int set non-zero when a
+ *     bounded wait expires (the output is then invalid).
+ */
+int vqc_ozaki_slice_rows(const double* src, int32_t nmol, int64_t rows, int32_t cols, int64_t ld,
+                         int64_t mol_stride, const double* col_scale, int32_t nslices, int8_t* dst,
+                         int32_t ldd, int32_t* exps, void* stream);
+int vqc_ozaki_gemm(const int8_t* a_slices, const int32_t* a_exps, int64_t m, const int8_t* b_slices,
+                   const int32_t* b_exps, int32_t n, int32_t k, int32_t ldk, int32_t nmol,
+                   int32_t nslices, int32_t upper, double* c, int64_t ldc, int64_t c_mol_stride,
+                   int32_t* error, void* stream);
 
 /*
  * One SP2 purification step for nmol molecules of one size n (row-major n*n

@@ -17,6 +17,7 @@ ABI_VERSION = 1
 STATUS = {
     0: "success",
     1: "invalid argument",
+    2: "ABI mismatch",
     4: "not converged",
     5: "numerical failure",
     6: "CUDA error",
@@ -70,6 +71,23 @@ class MoleculeInfo(ctypes.Structure):
     ]
 
 
+class DfGradientResources(ctypes.Structure):
+    """``vqc_df_gradient_resources`` (reference ``generativeqc_df_gradient_resources``)."""
+
+    _fields_ = [
+        ("struct_size", ctypes.c_uint32),
+        ("abi_version", ctypes.c_uint32),
+        ("host_bytes", ctypes.c_uint64),
+        ("device_bytes", ctypes.c_uint64),
+        ("host_to_device_bytes", ctypes.c_uint64),
+        ("device_to_host_bytes", ctypes.c_uint64),
+        ("weight_tile_elements", ctypes.c_uint64),
+        ("tiles", ctypes.c_uint64),
+        ("uploads", ctypes.c_uint64),
+        ("stream_synchronizations", ctypes.c_uint64),
+    ]
+
+
 # name -> argtypes (every function returns int status unless listed below)
 _P = ctypes.c_void_p
 _SIGNATURES = {
@@ -86,6 +104,15 @@ _SIGNATURES = {
     "vqc_grad3c": ([_P, _P, _P, _P, _P], ctypes.c_int),
     "vqc_grad2c": ([_P, _P, _P, _P, _P], ctypes.c_int),
     "vqc_grad1e": ([_P, _P, _P, _P, _P, _P], ctypes.c_int),
+    "vqc_df_gradient": ([ctypes.POINTER(BatchDesc), _P, _P, ctypes.c_size_t, _P, ctypes.c_size_t,
+                         ctypes.c_uint32, ctypes.c_size_t, ctypes.c_size_t, _P, ctypes.c_size_t,
+                         ctypes.POINTER(DfGradientResources)], ctypes.c_int),
+    "vqc_ozaki_slice_rows": ([_P, ctypes.c_int32, ctypes.c_int64, ctypes.c_int32, ctypes.c_int64,
+                              ctypes.c_int64, _P, ctypes.c_int32, _P, ctypes.c_int32, _P, _P],
+                             ctypes.c_int),
+    "vqc_ozaki_gemm": ([_P, _P, ctypes.c_int64, _P, _P, ctypes.c_int32, ctypes.c_int32,
+                        ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _P,
+                        ctypes.c_int64, ctypes.c_int64, _P, _P], ctypes.c_int),
     "vqc_sp2_update": ([_P, _P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
                         ctypes.c_double, _P, _P], ctypes.c_int),
     "vqc_unpack_aux_major": ([_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,

@@ -184,7 +184,14 @@ class PreparedBatch:
             raise ValueError("charges and multiplicities must match the ragged batch size")
         self._calc = calculator
         self._closed = False
-        self._warm_start = warm_start
+        # warm starts (reference python/generativeqc/batch.py:123-130,1376-1390):
+        # the converged density of each item's last successful execution seeds
+        # its next one; updates can be frozen for reproducible replays
+        self._warm_start = bool(warm_start)
+        self._warm_updates = True
+        self._warm: list = [None] * len(systems)  # device (N, N) densities
+        self._warm_origin: list = [None] * len(systems)  # "execution" or "checkpoint"
+        self._source_coordinates: list = [None] * len(systems)  # where each density converged
         self.charges = tuple(int(q) for q in charges)
         self.multiplicities = tuple(int(m) for m in mults)
         self._molecules = []
@@ -249,21 +256,78 @@ class PreparedBatch:
             out.append(arr)
         return out
 
+    # -- warm starts -------------------------------------------------------
+
+    def set_warm_start_updates(self, enabled: bool) -> None:
+        """Whether successful executions replace the retained densities.
+
+        Disabling updates freezes the current snapshots (warm starts stay on),
+        so every replay begins from the same densities.
+        """
+        self._warm_updates = bool(enabled)
+
+    def clear_warm_starts(self) -> None:
+        """Forget every retained density: the next execution starts cold."""
+        self._warm = [None] * len(self._molecules)
+        self._warm_origin = [None] * len(self._molecules)
+
+    def warm_start_available(self, index: int) -> bool:
+        return self._warm_start and self._warm[index] is not None
+
+    def _chunk_warm(self, chunk):
+        if not self._warm_start or all(self._warm[i] is None for i in chunk.indices):
+            return None, None
+        dev = self._calc.device
+        n = chunk.nao
+        dens = torch.zeros(chunk.nb, n, n, dtype=torch.float64, device=dev)
+        mask = torch.zeros(chunk.nb, dtype=torch.bool, device=dev)
+        for j, i in enumerate(chunk.indices):
+            if self._warm[i] is not None:
+                dens[j] = self._warm[i]
+                mask[j] = True
+        return dens, mask
+
+    def _retain(self, chunk, density: torch.Tensor, converged, coords, skip=()) -> None:
+        if not (self._warm_start and self._warm_updates):
+            return
+        for j, i in enumerate(chunk.indices):
+            if bool(converged[j]) and i not in skip:
+                self._warm[i] = density[j].detach().clone()
+                self._warm_origin[i] = "execution"
+                c = coords[i]
+                self._source_coordinates[i] = (c.detach().cpu().numpy() if torch.is_tensor(c)
+                                               else np.asarray(c, dtype=np.float64)).copy()
+
+    def save_checkpoint(self, path, *, max_bytes: int = 256 << 20) -> dict:
+        """Atomically write the retained densities (reference ``batch.py:1312``)."""
+        from .checkpoint import save_checkpoint
+
+        return save_checkpoint(self, path, max_bytes=max_bytes)
+
+    def load_checkpoint(self, path, *, allow_warm: bool = False, strict: bool = True,
+                        max_bytes: int = 256 << 20) -> dict:
+        """Seed the next execution from a checkpoint (reference ``batch.py:1324``)."""
+        from .checkpoint import load_checkpoint
+
+        return load_checkpoint(self, path, allow_warm=allow_warm, strict=strict, max_bytes=max_bytes)
+
     def _run_chunk(self, chunk, xyz: torch.Tensor, want_forces: bool):
         """Integrals, SCF and (optionally) the gradient of one chunk, all on device."""
         calc = self._calc
         ints = compute_integrals(chunk.plan, xyz)
+        warm_density, warm_mask = self._chunk_warm(chunk)
         out = run_scf(chunk, ints, xyz, precision=chunk.precision,
                       max_iterations=calc.max_iterations,
                       energy_tolerance=calc.energy_tolerance,
                       density_tolerance=calc.density_tolerance,
                       diis_history=calc.diis_history,
-                      relative_threshold=calc.relative_threshold)
+                      relative_threshold=calc.relative_threshold,
+                      warm_density=warm_density, warm_mask=warm_mask)
         grad = df_rhf_gradient(chunk, ints, out, xyz) if want_forces else None
         # keep only per-molecule results; the chunk's B tensor and factors go
         mf = out.pop("metric")
         slim = {k: out[k] for k in ("energy", "converged", "iterations", "energy_change",
-                                    "density_rms", "density")}
+                                    "density_rms", "density", "warm_used", "warm_fallback")}
         slim["metric_rank"] = mf.rank
         slim["metric_condition"] = mf.condition
         slim["metric_kind"] = mf.kind
@@ -315,6 +379,7 @@ class PreparedBatch:
                 out, g = self._run_chunk(chunk, xyz, True)
                 if not bool(out["converged"].all()):
                     raise RuntimeError("SCF did not converge for a system of the batch")
+                self._retain(chunk, out["density"], out["converged"].cpu().numpy(), coordinates)
                 off = 0
                 for j, i in enumerate(chunk.indices):
                     energies[i] = out["energy"][j]
@@ -357,6 +422,9 @@ class PreparedBatch:
                 de = out["energy_change"].cpu().numpy()
                 drms = out["density_rms"].cpu().numpy()
                 g = grad.cpu().numpy() if grad is not None else None
+                used = out["warm_used"].cpu().numpy()
+                fallback = out["warm_fallback"].cpu().numpy()
+                self._retain(chunk, out["density"], conv, coords, skip=bad)
                 off = 0
                 for j, i in enumerate(chunk.indices):
                     na = self._natoms[i]
@@ -378,6 +446,8 @@ class PreparedBatch:
                         density_rms=float(drms[j]),
                         executed_backend="cuda",
                         bucket_id=bucket,
+                        warm_start_used=bool(used[j]),
+                        warm_start_fallback=bool(fallback[j]),
                         basis_metadata={"nao": chunk.nao, "naux": chunk.naux,
                                         "metric_rank": int(out["metric_rank"][j]),
                                         "metric_condition": float(out["metric_condition"][j]),

@@ -214,6 +214,7 @@ int Plan::build(const vqc_batch_desc& d) {
           cm3.push_back(ClassMol{m, pbeg[c][m], abeg[lc][m], acnt[lc][m], (int)tri, 0});
         }
         if ((st = add_class(cls3c, la, lb, lc, dpairs[c], cm3, slots3c(la, lb, lc, sph)))) return st;
+        if (!cm3.empty()) cls3c_host.push_back(cm3);
       }
       std::vector<ClassMol> cm2;
       for (int m = 0; m < nmol; ++m)
@@ -248,7 +249,7 @@ int vqc_plan_create(const vqc_batch_desc* desc, vqc_plan** out) {
   if (!desc || !out) return fail(VQC_STATUS_INVALID_ARGUMENT, "null argument");
   *out = nullptr;
   if (desc->struct_size < sizeof(vqc_batch_desc) || desc->abi_version != VQC_ABI_VERSION)
-    return fail(VQC_STATUS_INVALID_ARGUMENT, "descriptor struct_size/abi_version mismatch");
+    return fail(VQC_STATUS_ABI_MISMATCH, "descriptor struct_size/abi_version mismatch");
   if (desc->nmol <= 0 || !desc->mol_atom_offset || !desc->mol_shell_offset || !desc->mol_aux_offset)
     return fail(VQC_STATUS_INVALID_ARGUMENT, "empty batch");
   Plan* p = new Plan();

@@ -36,6 +36,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include "tc_common.cuh"
 #include "vqc_df.h"
 #include "vqc_plan.hpp"
 
@@ -44,65 +45,6 @@ namespace tc {
 
 constexpr int BM = 128;
 constexpr int BK = 32;  // FP32 elements per K-block: one 128-byte swizzle row
-constexpr unsigned long long kWaitNs = 2000000000ull;
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ unsigned long long globaltimer() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
-               : "memory");
-}
-
-// bounded wait; false on timeout (budget_ns of %globaltimer) or when *abort is set
-__device__ __forceinline__ bool mbar_wait_for(uint32_t bar, uint32_t parity, volatile int* abort,
-                                              unsigned long long budget_ns) {
-  const unsigned long long t0 = globaltimer();
-  while (true) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred P;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
-        "selp.b32 %0, 1, 0, P;\n\t}"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    if (ok) return true;
-    if (*abort) return false;
-    if (globaltimer() - t0 > budget_ns) return false;
-  }
-}
-
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort) {
-  return mbar_wait_for(bar, parity, abort, kWaitNs);
-}
-
-__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* tm, int c0, int c1,
-                                            int c2, uint32_t bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
-      "l"(reinterpret_cast<uint64_t>(tm)), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
-      : "memory");
-}
-
-// K-major, 128-byte swizzle, 8-row groups 1024 bytes apart (SBO), version 1
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
-  return (uint64_t)((addr & 0x3FFFFu) >> 4) | (1ull << 16) | (64ull << 32) | (1ull << 46) |
-         (2ull << 61);
-}
-
 template <int BN>
 __device__ __forceinline__ constexpr uint32_t instr_desc() {
   // D = F32 (bits 4-5 = 1), A = B = TF32 (2), both K-major, N >> 3, M >> 4
@@ -118,19 +60,6 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64
       "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
       "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
       : "memory");
-}
-
-__device__ __forceinline__ void mma_commit(uint32_t bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                   bar)
-               : "memory");
-}
-
-__device__ __forceinline__ void fence_before_sync() {
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void fence_after_sync() {
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 }
 
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
@@ -164,10 +93,6 @@ __device__ __forceinline__ void split4(float4& v, float4& lo) {
   h = rn_tf32(v.w); lo.w = rn_tf32(v.w - h); v.w = h;
 }
 
-
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
 
 // Shared control block behind the operand stages.
 struct Ctrl {
@@ -687,18 +612,6 @@ __global__ void split_tf32_kernel(const float* __restrict__ x, float* __restrict
 // host side
 // ---------------------------------------------------------------------------
 
-static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  if (!fn) {
-    cudaDriverEntryPointQueryResult q;
-    void* f = nullptr;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
-  }
-  return fn;
-}
-
 // 3-D FP32 tensor [batch][rows][ld] read as (k < kext, row < rows, batch) boxes of
 // BK x box_rows; elements with k >= kext or row >= rows read as zero.
 static int make_map(CUtensorMap* tm, const float* base, int kext, int ld, int rows, int batch,
@@ -716,12 +629,6 @@ static int make_map(CUtensorMap* tm, const float* base, int kext, int ld, int ro
                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(VQC_STATUS_CUDA_ERROR, "cuTensorMapEncodeTiled failed");
   return VQC_STATUS_SUCCESS;
-}
-
-static int sm_count() {
-  int sms = 148, dev = 0;
-  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  return sms;
 }
 
 template <int BN>

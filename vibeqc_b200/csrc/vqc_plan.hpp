@@ -38,6 +38,9 @@ struct Plan {
   KernelArgs args{};
 
   std::vector<ClassLaunch> cls1e, cls2c, cls3c;
+  // host copies of the per-molecule work entries of each cls3c launch (the
+  // tiled gradient entry re-slices them by auxiliary shell range)
+  std::vector<std::vector<ClassMol>> cls3c_host;
 
   int build(const vqc_batch_desc& d);
   ~Plan();

@@ -162,3 +162,49 @@ def df_rhf_gradient(chunk, ints, scf_out: dict, xyz: torch.Tensor) -> torch.Tens
         grad[off:off + na] += gn
         off += na
     return grad
+
+
+def df_gradient_host(molecule, bar_a, bar_m, *, spherical: bool = True,
+                     maximum_bytes: int = 1 << 32, maximum_tile_elements: int = 0,
+                     schedule: int = 0, out=None):
+    """DF part of an energy gradient from fixed external weights, host in and out.
+
+    The contract of the reference's ``generativeqc_system_df_gradient_cuda``
+    (``include/generativeqc/generativeqc.h:1312-1333``) through
+    ``vqc_df_gradient``: ``bar_a`` full (N, N, X) and ``bar_m`` full (X, X)
+    FP64 arrays (either may be None for a zero channel; nonsymmetric weights
+    are allowed and every element counts once), auxiliary functions in the
+    molecule's order (shells sorted by angular momentum).  Returns
+    ``(gradient (natom, 3), resources dict)``; when ``out`` is given the
+    gradient is written into it, and only on success.
+    """
+    import ctypes
+
+    import numpy as np
+
+    from .plan import batch_descriptor
+
+    desc, keep = batch_descriptor([molecule], spherical)
+    xyz = np.ascontiguousarray(molecule.coordinates, dtype=np.float64)
+    natom = xyz.shape[0]
+    a = None if bar_a is None else np.ascontiguousarray(bar_a, dtype=np.float64)
+    m = None if bar_m is None else np.ascontiguousarray(bar_m, dtype=np.float64)
+    from . import basis as bas
+
+    n = bas.count_functions(molecule.orbital_shells, spherical)
+    x = bas.count_functions(molecule.aux_shells, spherical)
+    count_a = n * n * x if a is None else a.size
+    count_m = x * x if m is None else m.size
+    grad = np.zeros((natom, 3)) if out is None else out
+    if grad.dtype != np.float64 or not grad.flags.c_contiguous or grad.size != 3 * natom:
+        raise ValueError("out must be a C-contiguous float64 array of 3 * natom values")
+    res = _lib.DfGradientResources()
+    res.struct_size = ctypes.sizeof(_lib.DfGradientResources)
+    res.abi_version = _lib.ABI_VERSION
+    ptr = lambda v: None if v is None else v.ctypes.data  # noqa: E731
+    _lib.call("vqc_df_gradient", ctypes.byref(desc), ptr(xyz), ptr(a), count_a, ptr(m), count_m,
+              schedule, maximum_bytes, maximum_tile_elements, grad.ctypes.data, grad.size,
+              ctypes.byref(res))
+    del keep
+    rec = {name: int(getattr(res, name)) for name, _ in _lib.DfGradientResources._fields_[2:]}
+    return grad.reshape(natom, 3), rec

@@ -70,47 +70,56 @@ class MoleculeLayout:
         return self.nao * (self.nao + 1) // 2
 
 
+def batch_descriptor(molecules: list[MoleculeSpec], spherical: bool = True):
+    """``vqc_batch_desc`` for ``molecules`` plus the host arrays it points into.
+
+    The arrays must outlive every native call that reads the descriptor.
+    """
+    atom_off, sh_off, aux_off = [0], [0], [0]
+    charges, sl, sa, sn, sp, pe, pc = [], [], [], [], [], [], []
+    al, aa, an, ap, ae, ac = [], [], [], [], [], []
+    natom = 0
+    for mol in molecules:
+        charges.extend(mol.atomic_numbers.astype(np.float64))
+        for shells, l_, a_, n_, p_, e_, c_ in (
+            (mol.orbital_shells, sl, sa, sn, sp, pe, pc),
+            (mol.aux_shells, al, aa, an, ap, ae, ac),
+        ):
+            for s in shells:
+                ex, co = bas.normalized_coefficients(s)
+                l_.append(s.angular_momentum)
+                a_.append(natom + s.atom_index)
+                n_.append(len(ex))
+                p_.append(len(e_))
+                e_.extend(ex)
+                c_.extend(co)
+        natom += len(mol.atomic_numbers)
+        atom_off.append(natom)
+        sh_off.append(len(sl))
+        aux_off.append(len(al))
+    keep = [
+        _lib.i32(atom_off), _lib.i32(sh_off), _lib.i32(aux_off), _lib.f64(charges),
+        _lib.i32(sl), _lib.i32(sa), _lib.i32(sn), _lib.i32(sp), _lib.f64(pe), _lib.f64(pc),
+        _lib.i32(al), _lib.i32(aa), _lib.i32(an), _lib.i32(ap), _lib.f64(ae), _lib.f64(ac),
+    ]
+    k = keep
+    ptr = lambda a: a.ctypes.data  # noqa: E731
+    desc = _lib.BatchDesc(
+        ctypes.sizeof(_lib.BatchDesc), _lib.ABI_VERSION, len(molecules), int(spherical),
+        ptr(k[0]), ptr(k[1]), ptr(k[2]), ptr(k[3]),
+        ptr(k[4]), ptr(k[5]), ptr(k[6]), ptr(k[7]), ptr(k[8]), ptr(k[9]), len(pe),
+        ptr(k[10]), ptr(k[11]), ptr(k[12]), ptr(k[13]), ptr(k[14]), ptr(k[15]), len(ae),
+    )
+    return desc, keep
+
+
 class NativePlan:
     """Owns a ``vqc_plan`` for a fixed batch topology."""
 
     def __init__(self, molecules: list[MoleculeSpec], spherical: bool = True):
         self.molecules = molecules
         self.spherical = spherical
-        atom_off, sh_off, aux_off = [0], [0], [0]
-        charges, sl, sa, sn, sp, pe, pc = [], [], [], [], [], [], []
-        al, aa, an, ap, ae, ac = [], [], [], [], [], []
-        natom = 0
-        for mol in molecules:
-            charges.extend(mol.atomic_numbers.astype(np.float64))
-            for shells, l_, a_, n_, p_, e_, c_ in (
-                (mol.orbital_shells, sl, sa, sn, sp, pe, pc),
-                (mol.aux_shells, al, aa, an, ap, ae, ac),
-            ):
-                for s in shells:
-                    ex, co = bas.normalized_coefficients(s)
-                    l_.append(s.angular_momentum)
-                    a_.append(natom + s.atom_index)
-                    n_.append(len(ex))
-                    p_.append(len(e_))
-                    e_.extend(ex)
-                    c_.extend(co)
-            natom += len(mol.atomic_numbers)
-            atom_off.append(natom)
-            sh_off.append(len(sl))
-            aux_off.append(len(al))
-        self._keep = [
-            _lib.i32(atom_off), _lib.i32(sh_off), _lib.i32(aux_off), _lib.f64(charges),
-            _lib.i32(sl), _lib.i32(sa), _lib.i32(sn), _lib.i32(sp), _lib.f64(pe), _lib.f64(pc),
-            _lib.i32(al), _lib.i32(aa), _lib.i32(an), _lib.i32(ap), _lib.f64(ae), _lib.f64(ac),
-        ]
-        k = self._keep
-        ptr = lambda a: a.ctypes.data  # noqa: E731
-        desc = _lib.BatchDesc(
-            ctypes.sizeof(_lib.BatchDesc), _lib.ABI_VERSION, len(molecules), int(spherical),
-            ptr(k[0]), ptr(k[1]), ptr(k[2]), ptr(k[3]),
-            ptr(k[4]), ptr(k[5]), ptr(k[6]), ptr(k[7]), ptr(k[8]), ptr(k[9]), len(pe),
-            ptr(k[10]), ptr(k[11]), ptr(k[12]), ptr(k[13]), ptr(k[14]), ptr(k[15]), len(ae),
-        )
+        desc, self._keep = batch_descriptor(molecules, spherical)
         handle = ctypes.c_void_p()
         _lib.call("vqc_plan_create", ctypes.byref(desc), ctypes.byref(handle))
         self.handle = handle

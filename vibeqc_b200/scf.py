@@ -156,6 +156,10 @@ DOUBLE_EPS = 2.220446049250313e-16
 MIXED_ITERATION_CAP = 40  # plain tensor-core iterations before the anchor is forced
 ANCHOR_COMMUTATOR = 1e-5  # max|FDS - SDF| at which the FP64 anchor is formed
 ANCHOR_DIIS_RESET = False  # restart DIIS at the anchor
+# anchored builds after which a chunk that has not converged is re-anchored
+# (a fresh FP64 build at the current density): the increments' split-precision
+# error scales with |D - D0|, so a stalled chunk converges to FP64 noise
+REANCHOR_EVERY = 8
 
 
 def exact_energy(jk, d: torch.Tensor, c: torch.Tensor, h: torch.Tensor,
@@ -384,6 +388,9 @@ def occupied_factor(proj: torch.Tensor, guess: torch.Tensor, gen: torch.Generato
 
 
 WHITEN_COLUMN_BLOCK = 256
+# the mixed path whitens on the int8 tensor cores (whiten_tensor_cores); the
+# FP64 comparator path keeps plain FP64 GEMMs (whiten_in_place)
+WHITEN_TENSOR_CORES = os.environ.get("VQC_WHITEN_TC", "1") != "0"
 
 
 def whiten_in_place(a: torch.Tensor, mf: MetricFactor) -> None:
@@ -411,6 +418,64 @@ def whiten_in_place(a: torch.Tensor, mf: MetricFactor) -> None:
         for c0 in range(((x - 1) // cb) * cb, -1, -cb):
             c1 = min(x, c0 + cb)
             rows[:, :, c0:c1].copy_(torch.matmul(rows[:, :, :c1], w[:, :c1, c0:c1]))
+
+
+OZAKI_SLICES = 7  # 7-bit int8 slices per FP64 operand of the tensor-core whitening
+OZAKI_GROUP_BYTES = 4 << 30  # bound on the A-slice workspace (rows are sliced in groups)
+OZAKI_STATS = {"launches": 0, "int8_macs": 0}  # tensor-core whitening work since process start
+
+
+def whiten_tensor_cores(a: torch.Tensor, mf: MetricFactor, metric: torch.Tensor) -> None:
+    """B = A W over the packed rows of every molecule, in place, on the int8 tensor cores.
+
+    FP64 accuracy from exact integer pieces (vqc_ozaki_slice_rows /
+    vqc_ozaki_gemm): rows of A and columns of W are scaled by powers of two
+    and cut into OZAKI_SLICES 7-bit slices; the slice products accumulate
+    exactly in int32 and only their FP64 recombination rounds.  Before
+    slicing, A W = (A S)(S^-1 W) with S_i = 2^round(log2 sqrt(max_c |W_ic| /
+    sqrt(M_ii))) balances the column scale of A (|(mu nu|P)| <= sqrt((mu nu|mu nu)
+    M_PP) by the Schwarz inequality) against the row scale of W; powers of two
+    keep the rescaling exact.  With the Cholesky factor W = L^-T is upper
+    triangular and each output column tile reads only the rows of W above it.
+    The rows of A are sliced and multiplied in groups (slice workspace <=
+    OZAKI_GROUP_BYTES); a group's FP64 rows are overwritten only after they
+    were sliced.  Relative error ~1e-11 of each row's largest element at 7
+    slices; the resulting Coulomb/exchange energies differ from the FP64
+    product by ~1e-11 of their size.
+    """
+    nb, p_rows, x = a.shape
+    dev = a.device
+    ns = OZAKI_SLICES
+    w = mf.inv_sqrt
+    diag = torch.diagonal(metric, dim1=1, dim2=2).clamp_min(1e-300)
+    wmax = w.abs().amax(dim=2).clamp_min(1e-300)
+    scale = torch.exp2(torch.round(0.5 * (torch.log2(wmax) - 0.5 * torch.log2(diag)))).contiguous()
+    wt = (w / scale[:, :, None]).transpose(1, 2).contiguous()  # [c][i] = W[i][c] / S_i
+    ldk = (x + 15) // 16 * 16
+    st = _stream_ptr()
+    b_sl = torch.empty(nb, ns, x, ldk, dtype=torch.int8, device=dev)
+    b_exp = torch.empty(nb, x, dtype=torch.int32, device=dev)
+    _lib.call("vqc_ozaki_slice_rows", wt.data_ptr(), nb, x, x, x, x * x, None, ns, b_sl.data_ptr(),
+              ldk, b_exp.data_ptr(), st)
+    del wt
+    grp = max(128, (OZAKI_GROUP_BYTES // (nb * ns * ldk)) // 128 * 128)
+    grp = min(grp, p_rows)
+    a_sl = torch.empty(nb * ns * grp * ldk, dtype=torch.int8, device=dev)
+    a_exp = torch.empty(nb * grp, dtype=torch.int32, device=dev)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    upper = 1 if mf.kind == "cholesky" else 0
+    assert a.is_contiguous()
+    for r0 in range(0, p_rows, grp):
+        m = min(p_rows, r0 + grp) - r0
+        base = a.data_ptr() + r0 * x * 8
+        _lib.call("vqc_ozaki_slice_rows", base, nb, m, x, x, p_rows * x, scale.data_ptr(), ns,
+                  a_sl.data_ptr(), ldk, a_exp.data_ptr(), st)
+        _lib.call("vqc_ozaki_gemm", a_sl.data_ptr(), a_exp.data_ptr(), m, b_sl.data_ptr(),
+                  b_exp.data_ptr(), x, x, ldk, nb, ns, upper, base, x, p_rows * x, err.data_ptr(), st)
+        OZAKI_STATS["launches"] += 2
+        OZAKI_STATS["int8_macs"] += nb * m * x * x * ns * (ns + 1) // 2 // (2 if upper else 1)
+    if int(err.item()) != 0:
+        raise _lib.VqcError(6, f"tensor-core whitening wait expired (code {int(err.item())})")
 
 
 def _graphs_enabled() -> bool:
@@ -548,8 +613,19 @@ def _scf_post(nb, n, x, hist, with_rho, device) -> _SCFPost:
 def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision: str = "fp64",
             max_iterations: int = 100, energy_tolerance: float = 1e-10,
             density_tolerance: float = 1e-8, diis_history: int = 8,
-            relative_threshold: float = 1e-10, trace: list | None = None) -> dict:
-    """Batched SCF over one chunk; returns device tensors per molecule."""
+            relative_threshold: float = 1e-10, trace: list | None = None,
+            warm_density: torch.Tensor | None = None,
+            warm_mask: torch.Tensor | None = None) -> dict:
+    """Batched SCF over one chunk; returns device tensors per molecule.
+
+    ``warm_density`` (nb, N, N) with ``warm_mask`` (nb,) bool: molecules whose
+    mask is set start from the occupied space of that density (a converged
+    density of an earlier execution, possibly at another geometry) instead of
+    the core-Hamiltonian guess -- the same purification as the cold guess,
+    applied to F0 = -S D S / 2, whose lowest n_occ eigenvectors span the
+    S-orthogonalised occupied space of D.  A non-finite warm density falls
+    back to the cold guess (``warm_fallback``).
+    """
     nb, n, x, nocc = chunk.nb, chunk.nao, chunk.naux, chunk.nocc
     dev = xyz.device
     with TIMER.stage("metric_factor"):
@@ -557,7 +633,10 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
     with TIMER.stage("whiten"):
         b_packed = ints.a_packed  # whitened in place: B = A W
         ints.a_packed = None  # the raw tensor is not needed after whitening
-        whiten_in_place(b_packed, mf)
+        if precision == "mixed" and WHITEN_TENSOR_CORES:
+            whiten_tensor_cores(b_packed, mf, ints.metric)
+        else:
+            whiten_in_place(b_packed, mf)
         jk = jkmod.make_builder(precision, b_packed, n, x, nocc)
         del b_packed
     s, h = ints.s, ints.h
@@ -587,7 +666,16 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
             co = occupied_factor(proj, guess, gen, noise_scale)  # orthonormal, orthogonal basis
         return 2.0 * (xo @ proj @ xo.transpose(1, 2)), co
 
-    d, co = density_from(h, guess)
+    warm_used = torch.zeros(nb, dtype=torch.bool, device=dev)
+    warm_fallback = torch.zeros(nb, dtype=torch.bool, device=dev)
+    f0 = h
+    if warm_density is not None and warm_mask is not None and bool(warm_mask.any()):
+        finite = torch.isfinite(warm_density).flatten(1).all(dim=1)
+        warm_used = warm_mask & finite
+        warm_fallback = warm_mask & ~finite
+        wd = torch.where(warm_used[:, None, None], warm_density, torch.zeros_like(h))
+        f0 = torch.where(warm_used[:, None, None], -0.5 * (s @ wd @ s), h)
+    d, co = density_from(f0, guess)
     c = xo @ co  # AO occupied factor, D = 2 C C^T
     active = torch.ones(nb, dtype=torch.bool, device=dev)
     e_old = torch.full((nb,), float("nan"), dtype=torch.float64, device=dev)
@@ -616,17 +704,23 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
     phase_iterations = 0
     co_anchor = None
     anchored = False
+    anchor_builds = 0
+    anchors = 0
     for it in range(1, max_iterations + 1):
         rho = None
         if phase == "exact":
             j, k = jk.build_exact(d, c)
         elif phase == "anchor":
+            if anchored and anchor_builds >= REANCHOR_EVERY:
+                anchored, co_anchor, anchor_builds = False, None, 0
             if not anchored:
                 j, k, rho = jk.anchor(d, c)
                 anchored = True
+                anchors += 1
             else:
                 j, k, rho = jk.build_incremental(d, c)
                 mixed_iterations += 1
+                anchor_builds += 1
         else:
             j, k = jk.build(d, c)
             mixed_iterations += 1
@@ -707,6 +801,7 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
         "energy": final_e, "converged": converged, "iterations": iters,
         "energy_change": final_de, "density_rms": final_drms, "density": d_final,
         "orbitals": c_final, "fock": f_final, "exact_half": exact_half,
-        "mixed_iterations": mixed_iterations,
+        "mixed_iterations": mixed_iterations, "anchors": anchors,
+        "warm_used": warm_used, "warm_fallback": warm_fallback,
         "metric": mf, "orthogonalizer": xo, "enuc": enuc, "charges": zs, "jk": jk,
     }
