@@ -92,6 +92,18 @@ uint32_t vqc_abi_version(void);
 /* Number of kernel launches this library has issued (process lifetime). */
 uint64_t vqc_launch_count(void);
 
+/*
+ * Tuning knobs read by the kernels' launchers (process-wide; set between
+ * launches, e.g. from an autotuned table per batch shape).  No counterpart
+ * in the reference, whose CUDA schedules come from build-time tuning
+ * manifests (python/generativeqc_compiler/integral/df_tuning/).
+ *   VQC_TUNE_GRAM_WAVES: the exchange Gram product splits its K range until
+ *     about this many CTAs per SM exist (1..64, default 2).
+ */
+enum { VQC_TUNE_GRAM_WAVES = 1, VQC_TUNE_COUNT = 2 };
+int vqc_tune_set(int32_t knob, int32_t value);
+int vqc_tune_get(int32_t knob, int32_t* value);
+
 /* Plan over a batch topology (generativeqc_batch_prepare, generativeqc.h:1435). */
 int vqc_plan_create(const vqc_batch_desc* desc, vqc_plan** out);
 int vqc_plan_destroy(vqc_plan* plan);

@@ -13,6 +13,7 @@ import numpy as np
 
 LIB_PATH = Path(__file__).resolve().with_name("libvqc_b200.so")
 ABI_VERSION = 1
+TUNE_GRAM_WAVES = 1
 
 STATUS = {
     0: "success",
@@ -94,6 +95,8 @@ _SIGNATURES = {
     "vqc_last_error": ([], ctypes.c_char_p),
     "vqc_abi_version": ([], ctypes.c_uint32),
     "vqc_launch_count": ([], ctypes.c_uint64),
+    "vqc_tune_set": ([ctypes.c_int32, ctypes.c_int32], ctypes.c_int),
+    "vqc_tune_get": ([ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
     "vqc_plan_create": ([ctypes.POINTER(BatchDesc), ctypes.POINTER(_P)], ctypes.c_int),
     "vqc_plan_destroy": ([_P], ctypes.c_int),
     "vqc_plan_totals": ([_P, _P, _P, _P, _P], ctypes.c_int),

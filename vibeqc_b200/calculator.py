@@ -19,7 +19,7 @@ from typing import Iterable, Sequence
 import numpy as np
 import torch
 
-from . import _lib
+from . import _lib, tuning
 from .gradient import df_rhf_gradient
 from .plan import make_molecule
 from .scf import Chunk, compute_integrals, run_scf
@@ -316,7 +316,8 @@ class PreparedBatch:
         calc = self._calc
         ints = compute_integrals(chunk.plan, xyz)
         warm_density, warm_mask = self._chunk_warm(chunk)
-        out = run_scf(chunk, ints, xyz, precision=chunk.precision,
+        schedule = tuning.active_table().lookup(chunk.nao, chunk.naux, chunk.nocc)
+        out = run_scf(chunk, ints, xyz, precision=chunk.precision, schedule=schedule,
                       max_iterations=calc.max_iterations,
                       energy_tolerance=calc.energy_tolerance,
                       density_tolerance=calc.density_tolerance,

@@ -22,6 +22,16 @@ namespace vqc {
 thread_local std::string g_last_error;
 std::atomic<unsigned long long> g_launches{0};
 
+// tuning knobs: process-wide, read at launch time; values are checked against
+// each knob's range when set
+static std::atomic<int> g_tune[VQC_TUNE_COUNT] = {0, 2};
+static const int kTuneMin[VQC_TUNE_COUNT] = {0, 1};
+static const int kTuneMax[VQC_TUNE_COUNT] = {0, 64};
+
+int tune_value(int knob) {
+  return (knob > 0 && knob < VQC_TUNE_COUNT) ? g_tune[knob].load(std::memory_order_relaxed) : 0;
+}
+
 int fail(int status, const std::string& msg) {
   g_last_error = msg;
   return status;
@@ -243,6 +253,20 @@ extern "C" {
 const char* vqc_last_error(void) { return g_last_error.c_str(); }
 uint32_t vqc_abi_version(void) { return VQC_ABI_VERSION; }
 uint64_t vqc_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+int vqc_tune_set(int32_t knob, int32_t value) {
+  if (knob <= 0 || knob >= VQC_TUNE_COUNT || value < kTuneMin[knob] || value > kTuneMax[knob])
+    return fail(VQC_STATUS_INVALID_ARGUMENT, "tune_set: unknown knob or value out of range");
+  g_tune[knob].store(value, std::memory_order_relaxed);
+  return VQC_STATUS_SUCCESS;
+}
+
+int vqc_tune_get(int32_t knob, int32_t* value) {
+  if (knob <= 0 || knob >= VQC_TUNE_COUNT || !value)
+    return fail(VQC_STATUS_INVALID_ARGUMENT, "tune_get: unknown knob");
+  *value = g_tune[knob].load(std::memory_order_relaxed);
+  return VQC_STATUS_SUCCESS;
+}
 
 int vqc_plan_create(const vqc_batch_desc* desc, vqc_plan** out) {
   VQC_GUARD_BEGIN

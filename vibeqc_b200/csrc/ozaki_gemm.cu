@@ -20,11 +20,15 @@
 // there a cuBLAS FP64 GEMM), with the slice count chosen for the path's
 // accuracy.
 //
-//   ozaki_gemm_kernel: one 128 x 64 output tile per CTA; warp 0 issues TMA
-//   loads (per 128-byte K-block: the ns B-slice tiles as one group, then the
-//   ns A-slice tiles one by one), warp 1 issues the MMAs (for A slice s, the
-//   B slices t with s + t <= ns + 1 into accumulator g = s + t), warps 2-5
-//   drain the ns accumulators (TMEM -> int32 -> FP64) and store the tile.
+//   ozaki_gemm_kernel: one 128 x 64 output tile per CTA (the ns accumulators
+//   take 448 of the 512 TMEM columns, so one CTA per SM).  Per 128-byte
+//   K-block: warp 6 loads the ns B-slice tiles as one group (two groups in
+//   flight), warp 0 loads the ns A-slice tiles one by one (six in flight) in
+//   the interleaved order 0, ns-1, 1, ns-2, ... so that heavy (many pairs) and
+//   light slices alternate; warp 1 issues the MMAs (A slice s with the B
+//   slices t, s + t <= ns + 1, into accumulator g = s + t); warps 2-5 drain
+//   the accumulators (TMEM -> int32 -> FP64), scale, stage the tile in the
+//   idle A ring and store whole rows.
 //   With `upper`, B[n][k] = 0 for k > n and a column tile reads only the
 //   K-blocks below its last column.
 #include <algorithm>
@@ -42,12 +46,15 @@ constexpr int BM = 128;
 constexpr int BN = 64;
 constexpr int BKB = 128;  // K-block: 128 int8 = one 128-byte swizzle row = 4 MMA K-steps
 constexpr int kMaxSlices = 7;
-constexpr int kARing = 4;
+static_assert(BKB == 4 * 32, "the MMA issue loop is unrolled for four 32-byte K-steps per K-block");
+constexpr int kARing = 6;
 constexpr int kWRing = 2;
 constexpr int A_TILE = BM * BKB;              // 16 KB
 constexpr int B_TILE = BN * BKB;              // 8 KB
 constexpr int B_GROUP = kMaxSlices * B_TILE;  // 56 KB
-constexpr int kThreads = 192;                 // producer, MMA, four epilogue warps
+constexpr int kThreads = 224;  // A producer, MMA issuer, four epilogue warps, B producer
+constexpr int kStageLd = BN + 1;  // doubles per staged output row (padding against bank conflicts)
+static_assert(4 * 32 * kStageLd * 8 <= kARing * A_TILE, "epilogue staging fits in the A ring");
 constexpr int kTmemCols = 512;                // ns (<= 7) accumulators of BN columns
 
 struct OzCtrl {
@@ -101,6 +108,9 @@ __device__ __forceinline__ void tmem_ld16_i32(uint32_t taddr, int (&v)[16]) {
   for (int i = 0; i < 16; ++i) v[i] = (int)r[i];
 }
 
+// j-th A slice of a K-block in issue order: 0, ns-1, 1, ns-2, ...
+__device__ __forceinline__ int slice_order(int j, int ns) { return (j & 1) ? ns - 1 - (j >> 1) : (j >> 1); }
+
 // D = S32 (bits 4-5 = 2), A = B = signed 8-bit (1), both K-major, N >> 3, M >> 4
 constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
                               ((uint32_t)(BM >> 4) << 24);
@@ -152,9 +162,8 @@ __global__ void __launch_bounds__(kThreads, 1)
   const uint32_t tmem = ctrl->tmem;
   volatile int* ab = &ctrl->abort;
 
-  if (warp == 0) {
-    if (lane == 0) {  // TMA producer
-      int ai = 0;
+  if (warp == 6) {
+    if (lane == 0) {  // B-slice groups
       for (int kb = 0; kb < nkb && !oz_aborted(ctrl); ++kb) {
         const int ws = kb % kWRing;
         if (kb >= kWRing && !mbar_wait(be0 + 8 * ws, ((kb / kWRing) - 1) & 1, ab)) {
@@ -166,8 +175,14 @@ __global__ void __launch_bounds__(kThreads, 1)
           tma_load_3d(smem_u32(bbuf + ws * B_GROUP + t * B_TILE), &tmB, kb * BKB, n0, z * ns + t,
                       bf0 + 8 * ws);
         *reinterpret_cast<volatile int*>(&ctrl->b_issued) = kb + 1;
-        bool ok = true;
-        for (int s = 0; s < ns; ++s, ++ai) {
+      }
+    }
+  } else if (warp == 0) {
+    if (lane == 0) {  // A-slice tiles
+      int ai = 0;
+      bool ok = true;
+      for (int kb = 0; kb < nkb && ok && !oz_aborted(ctrl); ++kb) {
+        for (int j = 0; j < ns; ++j, ++ai) {
           const int as = ai % kARing;
           if (ai >= kARing && !mbar_wait(ae0 + 8 * as, ((ai / kARing) - 1) & 1, ab)) {
             oz_abort(ctrl, p.error, 42);
@@ -175,10 +190,10 @@ __global__ void __launch_bounds__(kThreads, 1)
             break;
           }
           mbar_expect_tx(af0 + 8 * as, A_TILE);
-          tma_load_3d(smem_u32(abuf + as * A_TILE), &tmA, kb * BKB, m0, z * ns + s, af0 + 8 * as);
+          tma_load_3d(smem_u32(abuf + as * A_TILE), &tmA, kb * BKB, m0, z * ns + slice_order(j, ns),
+                      af0 + 8 * as);
           *reinterpret_cast<volatile int*>(&ctrl->a_issued) = ai + 1;
         }
-        if (!ok) break;
       }
     }
   } else if (warp == 1) {
@@ -193,7 +208,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         *reinterpret_cast<volatile int*>(&ctrl->b_consumed) = kb + 1;
         const uint32_t bbase = smem_u32(bbuf + ws * B_GROUP);
-        for (int s = 0; s < ns; ++s, ++ai) {
+        for (int j = 0; j < ns; ++j, ++ai) {
+          const int s = slice_order(j, ns);
           const int as = ai % kARing;
           if (!mbar_wait(af0 + 8 * as, (ai / kARing) & 1, ab)) {
             oz_abort(ctrl, p.error, 44);
@@ -202,15 +218,25 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
           *reinterpret_cast<volatile int*>(&ctrl->a_consumed) = ai + 1;
           fence_after_sync();
-          const uint32_t abase = smem_u32(abuf + as * A_TILE);
           // slices are 0-based here: pair (s, t) with s + t <= ns - 1 feeds
-          // accumulator g = s + t (weight 2^-7(g+2))
-          for (int t = 0; t + s < ns; ++t) {
-            const uint32_t dt = tmem + (uint32_t)((s + t) * BN);
+          // accumulator g = s + t (weight 2^-7(g+2)).  Descriptors advance by
+          // 32 bytes (2 in the >> 4 address field) per MMA K-step and by one
+          // tile per B slice; the loop is unrolled so that one MMA issues every
+          // few instructions (each is ~32 tensor cycles of work).
+          const uint64_t ad = smem_desc(smem_u32(abuf + as * A_TILE));
+          const uint64_t bd0 = smem_desc(bbase);
+          const uint32_t acc0 = (kb == 0 && s == 0) ? 0u : 1u;
+          uint32_t dt = tmem + (uint32_t)(s * BN);
 #pragma unroll
-            for (int kk = 0; kk < BKB / 32; ++kk)
-              mma_i8(dt, smem_desc(abase + kk * 32), smem_desc(bbase + t * B_TILE + kk * 32),
-                     kIdescI8, (kb == 0 && s == 0 && kk == 0) ? 0u : 1u);
+          for (int t = 0; t < kMaxSlices; ++t) {
+            if (t + s < ns) {
+              const uint64_t bd = bd0 + (uint64_t)(t * (B_TILE >> 4));
+              mma_i8(dt, ad, bd, kIdescI8, acc0);
+              mma_i8(dt, ad + 2, bd + 2, kIdescI8, 1u);
+              mma_i8(dt, ad + 4, bd + 4, kIdescI8, 1u);
+              mma_i8(dt, ad + 6, bd + 6, kIdescI8, 1u);
+            }
+            dt += BN;
           }
           mma_commit(ae0 + 8 * as);
         }
@@ -221,7 +247,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   } else {  // epilogue warps 2..5: TMEM lane quarter (warp & 3)
     const int q = warp & 3;
-    const bool ok = __all_sync(0xffffffffu, mbar_wait(accf, 0, ab));
+    // the whole tile's MMAs run before this wait ends: poll with back-off
+    const bool ok = __all_sync(0xffffffffu, mbar_wait_backoff(accf, 0, ab, kWaitNs, 256));
     if (!ok) {
       if (lane == 0) oz_abort(ctrl, p.error, 45);
     } else {
@@ -240,15 +267,23 @@ __global__ void __launch_bounds__(kThreads, 1)
           for (int j = 0; j < 16; ++j) acc[c + j] = fma((double)v[j], scale, acc[c + j]);
         }
       }
-      if (row < p.m) {
-        const double ra = ldexp(1.0, p.a_exp[(long long)z * p.m + row]);
-        const int* eb = p.b_exp + (long long)z * p.n;
-        double* out = p.c + (long long)z * p.c_mol_stride + (long long)row * p.ldc;
+      // scale by 2^(ea + eb) in one step (no intermediate underflow), stage the
+      // warp's 32 rows in the idle A ring, then store whole rows
+      const int ea = row < p.m ? p.a_exp[(long long)z * p.m + row] : 0;
+      const int* eb = p.b_exp + (long long)z * p.n;
+      double* stage = reinterpret_cast<double*>(abuf) + (size_t)(warp - 2) * 32 * kStageLd;
 #pragma unroll
-        for (int c = 0; c < BN; ++c) {
-          const int col = n0 + c;
-          if (col < p.n) out[col] = acc[c] * ra * ldexp(1.0, eb[col]);
-        }
+      for (int c = 0; c < BN; ++c) {
+        const int col = n0 + c;
+        stage[lane * kStageLd + c] = col < p.n ? ldexp(acc[c], ea + eb[col]) : 0.0;
+      }
+      __syncwarp();
+      const int rbase = m0 + q * 32;
+      for (int r = 0; r < 32; ++r) {
+        if (rbase + r >= p.m) break;
+        double* out = p.c + (long long)z * p.c_mol_stride + (long long)(rbase + r) * p.ldc + n0;
+        if (n0 + lane < p.n) out[lane] = stage[r * kStageLd + lane];
+        if (n0 + 32 + lane < p.n) out[32 + lane] = stage[r * kStageLd + 32 + lane];
       }
     }
     fence_before_sync();

@@ -53,6 +53,27 @@ __device__ __forceinline__ bool mbar_wait_for(uint32_t bar, uint32_t parity, vol
   }
 }
 
+// bounded wait that sleeps between polls: for waiters that are not on the
+// critical path (they would otherwise steal issue slots from the warps that are)
+__device__ __forceinline__ bool mbar_wait_backoff(uint32_t bar, uint32_t parity, volatile int* abort,
+                                                  unsigned long long budget_ns, unsigned sleep_ns) {
+  const unsigned long long t0 = globaltimer();
+  while (true) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred P;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if (*abort) return false;
+    if (globaltimer() - t0 > budget_ns) return false;
+    __nanosleep(sleep_ns);
+  }
+}
+
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort) {
   return mbar_wait_for(bar, parity, abort, kWaitNs);
 }

@@ -730,7 +730,9 @@ static int launch_gram(const float* a_hi, const float* a_lo, const float* b_hi, 
   const int kb_total = (kdim + BK - 1) / BK * nseg;
   const int sms = sm_count();
   long long base = (long long)tiles * nmol;
-  int ksplit = (int)((2LL * sms + base - 1) / base);
+  // K ranges are split until about waves x SMs CTAs exist (a tuning knob)
+  const long long waves = tune_value(VQC_TUNE_GRAM_WAVES);
+  int ksplit = (int)((waves * sms + base - 1) / base);
   const int max_split = (kb_total + kGramFlush - 1) / kGramFlush;
   ksplit = ksplit < 1 ? 1 : (ksplit > max_split ? max_split : ksplit);
   int per = (kb_total + ksplit - 1) / ksplit;

@@ -46,6 +46,9 @@ struct Plan {
   ~Plan();
 };
 
+// current value of a tuning knob (vqc_tune_set; defaults in capi.cu)
+int tune_value(int knob);
+
 int fail(int status, const std::string& msg);
 void count_launch();
 int cuda_status(cudaError_t e, const char* where);

@@ -13,9 +13,15 @@ B[ij, Q] = sum_{mu nu} C[mu i] C[nu j] B[mu nu, Q].  The contractions with the
 derivative integrals run in the native kernels (vqc_grad3c/2c/1e); forces are
 F = -(g_1e + g_DF + dE_nn/dR) (``src/scf/rhf.cpp:856-868``).
 
-The full-rank form of Mbar is used; a metric whose eigenvalue cutoff removed
-functions is rejected for forces (numerical failure), as the thresholded
-spectral response needs the discarded components of the raw 3-centre tensor.
+At full rank Mbar = -Minv Mbar+ Minv.  When the eigenvalue cutoff removed
+auxiliary functions (rank < X), the energy depends on M through the
+thresholded pseudoinverse and Mbar is its spectral adjoint (Daleckii-Krein
+divided differences; reference ``src/integrals/density_fitting_metric.cpp:
+50-99`` and ``src/tensor/symmetric_matrix_function.cpp:62``), which needs
+Mbar+ in the raw basis, including the components along discarded
+eigenvectors: the raw 3-centre tensor is recomputed for such chunks.  An
+eigenvalue within 128 eps lambda_max of the cutoff is a rank crossing and the
+forces fail (numerical failure), as in the reference.
 """
 
 from __future__ import annotations
@@ -112,14 +118,55 @@ def chunk_weights(c: torch.Tensor, dens: torch.Tensor, rho: torch.Tensor, u: tor
 WEIGHT_GROUP_BYTES = 4 << 30  # molecules per batched weight group: ~4 GB of (o, N, X) temporaries
 
 
+DOUBLE_EPS = 2.220446049250313e-16
+
+
+def spectral_metric_adjoint(lam: torch.Tensor, vec: torch.Tensor, keep: torch.Tensor,
+                            mbar_plus: torch.Tensor, relative_threshold: float) -> torch.Tensor:
+    """Adjoint of M -> thresholded pseudoinverse for one molecule (FP64, on the device).
+
+    f(l) = 1/l on the retained eigenvalues and 0 on the discarded ones;
+    Mbar = V ((V^T Mbar+ V) o G) V^T with G_ij = (f(l_i) - f(l_j)) / (l_i - l_j)
+    and f' on (numerically) equal pairs.  Raises on an eigenvalue within
+    128 eps lambda_max of the cutoff (reference
+    ``density_fitting_metric.cpp:74-83``).
+    """
+    lmax = float(lam[-1])
+    cut = relative_threshold * lmax
+    if bool(((lam - cut).abs() <= 128 * DOUBLE_EPS * lmax).any()):
+        raise _lib.VqcError(5, "DF metric rank crossing: eigenvalue is unresolved at the cutoff")
+    safe = torch.where(keep, lam, torch.ones_like(lam))
+    fl = torch.where(keep, 1.0 / safe, torch.zeros_like(lam))
+    dl = lam[:, None] - lam[None, :]
+    same = dl.abs() <= 1e-14 * lmax
+    gam = (fl[:, None] - fl[None, :]) / torch.where(same, torch.ones_like(dl), dl)
+    deriv = torch.where(keep, -1.0 / (safe * safe), torch.zeros_like(lam))
+    gam = torch.where(same, 0.5 * (deriv[:, None] + deriv[None, :]), gam)
+    return vec @ ((vec.transpose(0, 1) @ mbar_plus @ vec) * gam) @ vec.transpose(0, 1)
+
+
+def _raw_mbar_plus(a_raw_packed: torch.Tensor, c: torch.Tensor, n: int) -> torch.Tensor:
+    """Mbar+ = rho rho^T / 2 - sum_ij A_ij A_ij^T in the raw auxiliary basis (one molecule).
+
+    A_ij[P] = sum_{mu nu} C[mu i] C[nu j] (mu nu|P), rho = sum D A = 2 sum_i A_ii.
+    """
+    x = a_raw_packed.shape[1]
+    o = c.shape[1]
+    a_full = a_raw_packed[unpack_index(n, a_raw_packed.device)]  # (N*N, X)
+    ui = (c.transpose(0, 1) @ a_full.view(n, n * x)).view(o, n, x)  # [i][nu][P]
+    del a_full
+    aij = torch.einsum("nj,inp->ijp", c, ui).reshape(o * o, x)
+    rho = 2.0 * aij.view(o, o, x).diagonal(dim1=0, dim2=1).sum(dim=1)
+    return 0.5 * torch.outer(rho, rho) - aij.transpose(0, 1) @ aij
+
+
 def df_rhf_gradient(chunk, ints, scf_out: dict, xyz: torch.Tensor) -> torch.Tensor:
     """Positive energy gradient, (natom_total_of_chunk, 3)."""
     plan = chunk.plan
     nb, n, x, o = chunk.nb, chunk.nao, chunk.naux, chunk.nocc
     dev = xyz.device
     mf = scf_out["metric"]
-    if any(r < x for r in mf.rank):
-        raise _lib.VqcError(5, "analytic forces need a full-rank auxiliary metric")
+    truncated = [m for m in range(nb) if mf.rank[m] < x]
     dens = scf_out["density"]
     c = scf_out["orbitals"]  # AO occupied factor, dens = 2 c c^T
     f = scf_out["fock"]
@@ -141,6 +188,19 @@ def df_rhf_gradient(chunk, ints, scf_out: dict, xyz: torch.Tensor) -> torch.Tens
         g1 = min(nb, g0 + grp)
         chunk_weights(c[g0:g1], dens[g0:g1], rho_all[g0:g1], u_all[g0:g1], mf.inv_sqrt[g0:g1], tri,
                       abar[g0:g1], mbar[g0:g1])
+    if truncated:
+        # the whitened tensor is no longer needed: recompute the raw one for
+        # the spectral response of the truncated metrics
+        del u_all
+        jk.release_all()
+        from .scf import compute_integrals
+
+        a_raw = compute_integrals(plan, xyz).a_packed
+        for m in truncated:
+            mbp = _raw_mbar_plus(a_raw[m], c[m], n)
+            mbar[m] = spectral_metric_adjoint(mf.eigenvalues[m], mf.eigenvectors[m], mf.keep[m], mbp,
+                                              scf_out["relative_threshold"])
+        del a_raw
     wctx.__exit__(None, None, None)
     grad = torch.zeros(plan.natom * 3, dtype=torch.float64, device=dev)
     st = torch.cuda.current_stream().cuda_stream

@@ -74,6 +74,10 @@ class FP64Builder:
         """(rho_whitened (nb, X), U (nb, N, o, X)) for D = 2 C C^T."""
         return fp64_half(self.b, c_occ, self.n, self.x)
 
+    def release_all(self) -> None:
+        """Drop the whitened tensor (no further builds)."""
+        self.b = None
+
 
 def fp64_half(b_full: torch.Tensor, c_occ: torch.Tensor, n: int, x: int):
     """FP64 U[mu][i][Q] = sum_nu B[mu nu, Q] C[nu, i] and rho = 2 sum C U.
@@ -176,6 +180,11 @@ class MixedBuilder:
         """FP64 (rho_whitened (nb, X), U (nb, N, o, X)) from the FP64 whitened tensor."""
         with TIMER.stage("exact_half_fp64"):
             return fp64_half(self.b64, c_occ, self.n, self.x)
+
+    def release_all(self) -> None:
+        """Drop every copy of the whitened tensor (no further builds)."""
+        self.release_tensor_core_buffers()
+        self.b64 = None
 
     def release_tensor_core_buffers(self) -> None:
         """Free the FP32 tensor and the split U/V buffers once the SCF is done."""

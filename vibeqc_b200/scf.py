@@ -219,7 +219,8 @@ class _SP2Graph:
     reads the device flags once per replay.
     """
 
-    def __init__(self, nb: int, n: int, nocc: int, tol: float, device):
+    def __init__(self, nb: int, n: int, nocc: int, tol: float, device, steps: int = SP2_GRAPH_STEPS):
+        self.steps = int(steps)
         self.x = torch.zeros(nb, n, n, dtype=torch.float64, device=device)
         self.x2 = torch.empty_like(self.x)
         self.xn = torch.empty_like(self.x)
@@ -238,10 +239,10 @@ class _SP2Graph:
             self._steps()
 
     def run(self):
-        """SP2_GRAPH_STEPS steps: one graph replay, or eager launches."""
+        """``steps`` steps: one graph replay, or eager launches."""
         if self.graph is not None:
             self.graph.replay()
-            GRAPH_LAUNCHES[0] += SP2_GRAPH_STEPS
+            GRAPH_LAUNCHES[0] += self.steps
         else:
             self._steps()
 
@@ -249,7 +250,7 @@ class _SP2Graph:
         nb, n, nocc, tol = self.args
         st = torch.cuda.current_stream().cuda_stream
         x, xn = self.x, self.xn
-        for _ in range(SP2_GRAPH_STEPS):
+        for _ in range(self.steps):
             torch.bmm(x, x, out=self.x2)
             _lib.call("vqc_sp2_update", x.data_ptr(), self.x2.data_ptr(), xn.data_ptr(), nb, n,
                       nocc, tol, self.done.data_ptr(), st)
@@ -263,7 +264,7 @@ SP2_GRAPH_CACHE_BYTES = 4 << 30  # drop the cache when its buffers would exceed 
 
 
 def purify_sp2(fo: torch.Tensor, nocc: int, max_steps: int = 96, tol: float = 1e-11,
-               graphs: dict | None = None) -> torch.Tensor:
+               graphs: dict | None = None, steps: int = SP2_GRAPH_STEPS) -> torch.Tensor:
     """Projector onto the lowest ``nocc`` eigenvectors of symmetric ``fo``.
 
     Second-order spectral projection (Niklasson, Phys. Rev. B 66, 155115
@@ -272,7 +273,8 @@ def purify_sp2(fo: torch.Tensor, nocc: int, max_steps: int = 96, tol: float = 1e
     tr(X) - tr(X^2) < tol.  Per step: one batched GEMM and one native update
     kernel (vqc_sp2_update); convergence flags stay on the device.  Steps run
     in CUDA graphs of SP2_GRAPH_STEPS (cached in ``graphs``, one per shape and
-    tolerance), and the flags are read once per graph replay.
+    tolerance), and the flags are read once per graph replay.  ``steps`` (even)
+    is the number of steps per graph (an autotuned schedule choice).
     """
     nb, n, _ = fo.shape
     diag = torch.diagonal(fo, dim1=1, dim2=2)
@@ -280,7 +282,7 @@ def purify_sp2(fo: torch.Tensor, nocc: int, max_steps: int = 96, tol: float = 1e
     emin = (diag - radius).min(dim=1).values
     emax = (diag + radius).max(dim=1).values
     eye = torch.eye(n, dtype=fo.dtype, device=fo.device)
-    key = (nb, n, int(nocc), float(tol), str(fo.device))
+    key = (nb, n, int(nocc), float(tol), str(fo.device), int(steps))
     if graphs is None:
         graphs = {}
     g = graphs.get(key)
@@ -288,10 +290,10 @@ def purify_sp2(fo: torch.Tensor, nocc: int, max_steps: int = 96, tol: float = 1e
         held = sum(3 * v.x.numel() * 8 for v in graphs.values())
         if held + 3 * nb * n * n * 8 > SP2_GRAPH_CACHE_BYTES:
             graphs.clear()
-        g = graphs[key] = _SP2Graph(nb, n, nocc, tol, fo.device)
+        g = graphs[key] = _SP2Graph(nb, n, nocc, tol, fo.device, steps)
     torch.div(emax[:, None, None] * eye - fo, (emax - emin)[:, None, None], out=g.x)
     g.done.zero_()
-    for _ in range(0, max_steps, SP2_GRAPH_STEPS):
+    for _ in range(0, max_steps, int(steps)):
         g.run()
         if bool(g.done.all()):
             break
@@ -615,7 +617,7 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
             density_tolerance: float = 1e-8, diis_history: int = 8,
             relative_threshold: float = 1e-10, trace: list | None = None,
             warm_density: torch.Tensor | None = None,
-            warm_mask: torch.Tensor | None = None) -> dict:
+            warm_mask: torch.Tensor | None = None, schedule=None) -> dict:
     """Batched SCF over one chunk; returns device tensors per molecule.
 
     ``warm_density`` (nb, N, N) with ``warm_mask`` (nb,) bool: molecules whose
@@ -624,8 +626,14 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
     the core-Hamiltonian guess -- the same purification as the cold guess,
     applied to F0 = -S D S / 2, whose lowest n_occ eigenvectors span the
     S-orthogonalised occupied space of D.  A non-finite warm density falls
-    back to the cold guess (``warm_fallback``).
+    back to the cold guess (``warm_fallback``).  ``schedule`` (a
+    ``tuning.Schedule``, default the untuned one) picks the whitening
+    kernels of the mixed path, the SP2 steps per graph and the Gram split.
     """
+    from .tuning import DEFAULT, apply_library_knobs
+
+    sched = DEFAULT if schedule is None else schedule
+    apply_library_knobs(sched)
     nb, n, x, nocc = chunk.nb, chunk.nao, chunk.naux, chunk.nocc
     dev = xyz.device
     with TIMER.stage("metric_factor"):
@@ -633,7 +641,7 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
     with TIMER.stage("whiten"):
         b_packed = ints.a_packed  # whitened in place: B = A W
         ints.a_packed = None  # the raw tensor is not needed after whitening
-        if precision == "mixed" and WHITEN_TENSOR_CORES:
+        if precision == "mixed" and WHITEN_TENSOR_CORES and sched.whiten == "int8":
             whiten_tensor_cores(b_packed, mf, ints.metric)
         else:
             whiten_in_place(b_packed, mf)
@@ -661,7 +669,8 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
 
     def density_from(f, guess, tol=1e-11, noise_scale=0.3):
         with TIMER.stage("purify"):
-            proj = purify_sp2(xo.transpose(1, 2) @ f @ xo, nocc, tol=tol, graphs=sp2_graphs)
+            proj = purify_sp2(xo.transpose(1, 2) @ f @ xo, nocc, tol=tol, graphs=sp2_graphs,
+                              steps=sched.sp2_steps)
         with TIMER.stage("occupied_factor"):
             co = occupied_factor(proj, guess, gen, noise_scale)  # orthonormal, orthogonal basis
         return 2.0 * (xo @ proj @ xo.transpose(1, 2)), co
@@ -804,4 +813,5 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
         "mixed_iterations": mixed_iterations, "anchors": anchors,
         "warm_used": warm_used, "warm_fallback": warm_fallback,
         "metric": mf, "orthogonalizer": xo, "enuc": enuc, "charges": zs, "jk": jk,
+        "relative_threshold": relative_threshold,
     }
