@@ -52,7 +52,9 @@ def test_truncated_metric_forces_match_oracle(drop, precision):
     res = calc.singlepoint(ATOMS)
     assert res.basis_metadata["metric_rank"] == ref.extra["rank"]
     assert abs(res.energy - ref.energy) < 1e-8
-    assert np.abs(res.forces - ref.forces).max() < 2e-7
+    # FP64: 2e-7 Eh/Bohr as for the reference goldens; mixed (split-precision
+    # products, anchored increments): 1e-6, ten times inside its 1e-5 target
+    assert np.abs(res.forces - ref.forces).max() < (2e-7 if precision == "fp64" else 1e-6)
     assert np.abs(res.forces.sum(axis=0)).max() < 1e-8
 
 

@@ -345,14 +345,26 @@ class PreparedBatch:
             for c in self._chunks
         ]
 
-    def execute_device(self, xyz_chunks: list, *, want_forces: bool = True) -> list:
+    def execute_device(self, xyz_chunks: list, *, want_forces: bool = True,
+                       chunk_events: list | None = None) -> list:
         """Device-resident execution: inputs and outputs stay in HBM.
 
         Returns, per chunk, ``(scf_output_dict, gradient_or_None)`` with device
-        tensors; no host copies are made.
+        tensors; no host copies are made.  With ``chunk_events`` (a list), a
+        (shape, start event, end event) triple per chunk is appended for
+        per-chunk device timing.
         """
+        out = []
         with torch.cuda.device(self._calc.device):
-            return [self._run_chunk(c, x, want_forces) for c, x in zip(self._chunks, xyz_chunks)]
+            for c, x in zip(self._chunks, xyz_chunks):
+                if chunk_events is not None:
+                    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    s.record()
+                out.append(self._run_chunk(c, x, want_forces))
+                if chunk_events is not None:
+                    e.record()
+                    chunk_events.append(((c.nao, c.naux, c.nocc, c.nb), s, e))
+        return out
 
     def execute_tensors(self, coordinates: list) -> tuple:
         """Energies and gradients for per-system coordinate tensors, on the device.

@@ -94,6 +94,24 @@ __device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t
       : "memory");
 }
 
+// 32 consecutive columns of a lane quarter, without waiting (tcgen05.wait::ld
+// follows once all loads of an accumulator are in flight)
+__device__ __forceinline__ void tmem_ld32_i32_nowait(uint32_t taddr, int* v) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+      "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
+      "%30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
+        "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
+        "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = (int)r[i];
+}
+
 __device__ __forceinline__ void tmem_ld16_i32(uint32_t taddr, int (&v)[16]) {
   uint32_t r[16];
   asm volatile(
@@ -219,24 +237,15 @@ __global__ void __launch_bounds__(kThreads, 1)
           *reinterpret_cast<volatile int*>(&ctrl->a_consumed) = ai + 1;
           fence_after_sync();
           // slices are 0-based here: pair (s, t) with s + t <= ns - 1 feeds
-          // accumulator g = s + t (weight 2^-7(g+2)).  Descriptors advance by
-          // 32 bytes (2 in the >> 4 address field) per MMA K-step and by one
-          // tile per B slice; the loop is unrolled so that one MMA issues every
-          // few instructions (each is ~32 tensor cycles of work).
-          const uint64_t ad = smem_desc(smem_u32(abuf + as * A_TILE));
-          const uint64_t bd0 = smem_desc(bbase);
-          const uint32_t acc0 = (kb == 0 && s == 0) ? 0u : 1u;
-          uint32_t dt = tmem + (uint32_t)(s * BN);
+          // accumulator g = s + t (weight 2^-7(g+2)); four 32-byte K-steps per
+          // K-block (measured faster than a fully unrolled form)
+          const uint32_t abase = smem_u32(abuf + as * A_TILE);
+          for (int t = 0; t + s < ns; ++t) {
+            const uint32_t dt = tmem + (uint32_t)((s + t) * BN);
 #pragma unroll
-          for (int t = 0; t < kMaxSlices; ++t) {
-            if (t + s < ns) {
-              const uint64_t bd = bd0 + (uint64_t)(t * (B_TILE >> 4));
-              mma_i8(dt, ad, bd, kIdescI8, acc0);
-              mma_i8(dt, ad + 2, bd + 2, kIdescI8, 1u);
-              mma_i8(dt, ad + 4, bd + 4, kIdescI8, 1u);
-              mma_i8(dt, ad + 6, bd + 6, kIdescI8, 1u);
-            }
-            dt += BN;
+            for (int kk = 0; kk < BKB / 32; ++kk)
+              mma_i8(dt, smem_desc(abase + kk * 32), smem_desc(bbase + t * B_TILE + kk * 32),
+                     kIdescI8, (kb == 0 && s == 0 && kk == 0) ? 0u : 1u);
           }
           mma_commit(ae0 + 8 * as);
         }
@@ -259,13 +268,13 @@ __global__ void __launch_bounds__(kThreads, 1)
       for (int c = 0; c < BN; ++c) acc[c] = 0.0;
       double scale = 1.0 / 16384.0;  // 2^-7g for g = 2
       for (int g = 0; g < ns; ++g, scale *= 1.0 / 128.0) {
+        int v[BN];
+        const uint32_t ta = tmem + (uint32_t)(g * BN) + ((uint32_t)(q * 32) << 16);
+        tmem_ld32_i32_nowait(ta, v);
+        tmem_ld32_i32_nowait(ta + 32, v + 32);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-        for (int c = 0; c < BN; c += 16) {
-          int v[16];
-          tmem_ld16_i32(tmem + (uint32_t)(g * BN + c) + ((uint32_t)(q * 32) << 16), v);
-#pragma unroll
-          for (int j = 0; j < 16; ++j) acc[c + j] = fma((double)v[j], scale, acc[c + j]);
-        }
+        for (int c = 0; c < BN; ++c) acc[c] = fma((double)v[c], scale, acc[c]);
       }
       // scale by 2^(ea + eb) in one step (no intermediate underflow), stage the
       // warp's 32 rows in the idle A ring, then store whole rows
