@@ -39,7 +39,7 @@ from oracle import oracle  # noqa: E402
 from vibeqc_b200 import geometry  # noqa: E402
 
 OUT = HERE / "oracle_workload_fixtures.json"
-CLUSTER_SIZES = tuple(range(2, 13))
+CLUSTER_SIZES = tuple(range(2, 17))
 ALKANE_SIZES = (4, 5, 6, 8)
 
 

@@ -1,6 +1,6 @@
 """Workload molecules on the GPU against fixtures and finite differences.
 
-* Water clusters (H2O)n, n = 2..12, taken from the 256-cluster ragged workload
+* Water clusters (H2O)n, n = 2..16 (one per size), taken from the 256-cluster ragged workload
   (def2-SVP / cc-pVDZ-JKFIT), and alkanes C4-C8 from the 64-alkane workload
   (def2-SVP / def2-TZVP): FP64 and mixed-precision energies and forces against
   ``oracle_workload_fixtures.json`` (CPU oracle, itself pinned against the
