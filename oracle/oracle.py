@@ -399,3 +399,144 @@ def df_rhf_gradient(orb, aux, xyz, z, a, mf, d, coef, e_mo, nocc, gnuc, relative
     g += grad2c(aux, xyz, mbar)
     g += gnuc
     return g
+
+
+# --------------------------------------------------------------------------
+# DF-UHF
+# --------------------------------------------------------------------------
+
+
+def build_k(b: np.ndarray, d: np.ndarray) -> np.ndarray:
+    """Density-form exchange K[D] = sum_Q B_Q D B_Q from whitened B (N, N, X)."""
+    bq = np.ascontiguousarray(b.transpose(2, 0, 1))
+    return np.einsum("qml,ls,qsn->mn", bq, d, bq, optimize=True)
+
+
+def spin_counts(nelectron: int, multiplicity: int) -> tuple[int, int]:
+    """(n_alpha, n_beta) for a total electron count and spin multiplicity 2S+1."""
+    if multiplicity < 1 or (nelectron + multiplicity - 1) % 2:
+        raise ValueError("electron count and multiplicity are inconsistent")
+    na = (nelectron + multiplicity - 1) // 2
+    nb = nelectron - na
+    if nb < 0:
+        raise ValueError("multiplicity exceeds the electron count")
+    return na, nb
+
+
+def df_uhf(atoms, basis="def2-svp", auxiliary_basis="cc-pvdz-jkfit", *, spherical=True,
+           charge=0, multiplicity=2, max_iterations=100, energy_tolerance=1e-10,
+           density_tolerance=1e-8, diis_history=8, forces=True,
+           relative_threshold=1e-10) -> OracleResult:
+    """Unrestricted DF-HF energy and analytic forces.
+
+    F_s = H + J[D_a + D_b] - K[D_s] (reference ``src/scf/density_fitting.cpp:844``),
+    E = 1/2 tr(D_t H) + 1/2 sum_s tr(D_s F_s) + E_nn; Pulay DIIS with one set of
+    weights over both spins' residuals F_s D_s S - S D_s F_s (reference
+    ``src/scf/cuda/df_scf_diis.cpp:110-185``); convergence on |dE|, the rms of
+    both spin-density changes and the larger spin residual
+    (``src/scf/cuda/df_scf_kernels.cu:296-340``).
+    """
+    z, xyz = molecule_arrays(atoms)
+    orb_sh = bas.expand_shells(z.astype(int), basis)
+    aux_sh = bas.expand_shells(z.astype(int), auxiliary_basis)
+    orb, aux = OracleBasis(orb_sh, spherical), OracleBasis(aux_sh, spherical)
+    na, nb = spin_counts(int(z.sum()) - charge, multiplicity)
+    s, t, v = int1e(orb, xyz, z)
+    h = t + v
+    m = int2c(aux, xyz)
+    a = int3c(orb, aux, xyz)
+    mf = factor_metric(m, relative_threshold)
+    b = a @ mf.inv_sqrt
+    enuc, gnuc = nuclear_repulsion(xyz, z)
+    sl, sv = np.linalg.eigh(s)
+    xorth = (sv / np.sqrt(sl)) @ sv.T
+    occ = (na, nb)
+
+    def densities_from(fs):
+        out = []
+        for f, n in zip(fs, occ):
+            e, cp = np.linalg.eigh(xorth.T @ f @ xorth)
+            c = xorth @ cp
+            out.append((c[:, :n] @ c[:, :n].T, e, c))
+        return out
+
+    ds = [x[0] for x in densities_from((h, h))]
+    e_old = None
+    errs, focks = [], []
+    converged = False
+    it = 0
+    for it in range(1, max_iterations + 1):
+        j = build_jk(b, ds[0] + ds[1])[0]
+        fs = [h + j - build_k(b, d) for d in ds]
+        energy = (0.5 * np.sum((ds[0] + ds[1]) * h)
+                  + 0.5 * sum(np.sum(d * f) for d, f in zip(ds, fs)) + enuc)
+        res = [f @ d @ s - s @ d @ f for d, f in zip(ds, fs)]
+        errs.append(np.concatenate([xorth.T @ r @ xorth for r in res]))
+        focks.append(fs)
+        errs, focks = errs[-diis_history:], focks[-diis_history:]
+        nh = len(errs)
+        f_ext = fs
+        if nh > 1:
+            bm = -np.ones((nh + 1, nh + 1))
+            bm[nh, nh] = 0.0
+            for i in range(nh):
+                for jj in range(nh):
+                    bm[i, jj] = np.sum(errs[i] * errs[jj])
+            rhs = np.zeros(nh + 1)
+            rhs[nh] = -1.0
+            try:
+                w = np.linalg.solve(bm, rhs)[:nh]
+                f_ext = [sum(wi * fk[sp] for wi, fk in zip(w, focks)) for sp in range(2)]
+            except np.linalg.LinAlgError:
+                f_ext = fs
+        new = [x[0] for x in densities_from(f_ext)]
+        de = abs(energy - e_old) if e_old is not None else np.inf
+        drms = float(np.sqrt(sum(np.sum((dn - d) ** 2) for dn, d in zip(new, ds))
+                             / (2 * ds[0].size)))
+        comm = max(float(np.abs(r).max()) for r in res)
+        guard = 16.0 * 2.220446049250313e-16 * max(1.0, abs(energy), abs(e_old or 0.0))
+        e_old = energy
+        if de < energy_tolerance + guard and drms < density_tolerance and comm <= min(1e-8, density_tolerance):
+            converged = True
+            break
+        ds = new
+    j = build_jk(b, ds[0] + ds[1])[0]
+    fs = [h + j - build_k(b, d) for d in ds]
+    energy = (0.5 * np.sum((ds[0] + ds[1]) * h)
+              + 0.5 * sum(np.sum(d * f) for d, f in zip(ds, fs)) + enuc)
+    result = OracleResult(energy, None, converged, it, ds[0] + ds[1], np.zeros(0),
+                          np.zeros((0, 0)), na, {"alpha_density": ds[0], "beta_density": ds[1],
+                                                  "nalpha": na, "nbeta": nb})
+    if forces:
+        result.forces = -df_uhf_gradient(orb, aux, xyz, z, a, mf, ds, fs, gnuc, relative_threshold)
+    result.extra.update(nao=orb.nfunc, naux=aux.nfunc, rank=mf.rank, condition=mf.condition)
+    return result
+
+
+def df_uhf_gradient(orb, aux, xyz, z, a, mf, ds, fs, gnuc, relative_threshold=1e-10):
+    """Positive energy gradient (natom, 3) of DF-UHF at its SCF solution.
+
+    Reverse weights as the reference's unrestricted weighted gradient
+    (``src/scf/density_fitting.cpp:919-944``: Coulomb on D_a + D_b, exchange
+    on each spin density with Fock coefficient -1): with rho = A:D_t,
+        Abar  = D_t (x) M+ rho - sum_s M+ (D_s A D_s),
+        Mbar+ = rho rho^T / 2 - 1/2 sum_s Q(D_s),  Q_PQ = A_P : (D_s A_Q D_s);
+    energy-weighted density W = sum_s D_s F_s D_s.
+    """
+    dt = ds[0] + ds[1]
+    wmat = sum(d @ f @ d for d, f in zip(ds, fs))
+    rho = np.einsum("mnp,mn->p", a, dt, optimize=True)
+    cvec = mf.pinv @ rho
+    aq = np.ascontiguousarray(a.transpose(2, 0, 1))
+    abar = dt[:, :, None] * cvec[None, None, :]
+    mbar_plus = 0.5 * np.outer(rho, rho)
+    for d in ds:
+        daq = np.einsum("ml,qls,sn->qmn", d, aq, d, optimize=True)
+        abar -= np.einsum("pq,qmn->mnp", mf.pinv, daq, optimize=True)
+        mbar_plus -= 0.5 * np.einsum("pmn,qmn->pq", aq, daq, optimize=True)
+    mbar = metric_response(mf, mbar_plus, relative_threshold)
+    g = grad1e(orb, xyz, z, dt, wmat)
+    g += grad3c(orb, aux, xyz, abar)
+    g += grad2c(aux, xyz, mbar)
+    g += gnuc
+    return g
