@@ -540,3 +540,55 @@ def df_uhf_gradient(orb, aux, xyz, z, a, mf, ds, fs, gnuc, relative_threshold=1e
     g += grad2c(aux, xyz, mbar)
     g += gnuc
     return g
+
+
+# --------------------------------------------------------------------------
+# Fixed-density DF J/K with declared Fock coefficients
+# --------------------------------------------------------------------------
+
+
+def fock_evaluate(atoms, basis, auxiliary_basis, densities, coulomb=1.0, exchange=-0.5, *,
+                  spherical=True, relative_threshold=1e-10, derivative=True) -> dict:
+    """J, K, Fock matrices, energies and dE2/dR at fixed AO densities.
+
+    Reference semantics (``src/scf/fock_build.cpp:429-495``, ``src/api/c_api_fock.cpp:
+    180-232``): ``densities`` is [D] (restricted, D the total density) or
+    [D_a, D_b] (unrestricted); J = J[D_a + D_b], K_s = K[D_s];
+    F_s = H + c_J J + c_K K_s; E1 = tr(D_t H);
+    E2 = 1/2 c_J tr(D_t J) + 1/2 c_K sum_s tr(D_s K_s); the gradient is dE2/dR
+    at fixed D through the DF reverse weights
+        Abar  = c_J D_t (x) M+ rho + c_K sum_s M+ (D_s A D_s),
+        Mbar+ = 1/2 c_J rho rho^T + 1/2 c_K sum_s Q(D_s).
+    """
+    z, xyz = molecule_arrays(atoms)
+    orb = OracleBasis(bas.expand_shells(z.astype(int), basis), spherical)
+    aux = OracleBasis(bas.expand_shells(z.astype(int), auxiliary_basis), spherical)
+    s, t, v = int1e(orb, xyz, z)
+    h = t + v
+    m = int2c(aux, xyz)
+    a = int3c(orb, aux, xyz)
+    mf = factor_metric(m, relative_threshold)
+    ds = [np.asarray(d, dtype=np.float64) for d in densities]
+    dt = sum(ds)
+    rho = np.einsum("mnp,mn->p", a, dt, optimize=True)
+    cvec = mf.pinv @ rho
+    j = a @ cvec
+    aq = np.ascontiguousarray(a.transpose(2, 0, 1))
+    ks = [np.einsum("pml,ls,qsn,pq->mn", aq, d, aq, mf.pinv, optimize=True) for d in ds]
+    fs = [h + coulomb * j + exchange * k for k in ks]
+    e1 = float(np.sum(dt * h))
+    e2 = 0.5 * coulomb * float(np.sum(dt * j)) + 0.5 * exchange * sum(
+        float(np.sum(d * k)) for d, k in zip(ds, ks))
+    enuc, _ = nuclear_repulsion(xyz, z)
+    out = {"coulomb": j, "exchange": ks, "fock": fs, "energy_one_electron": e1,
+           "energy_two_electron": e2, "nuclear_repulsion": enuc, "gradient": None}
+    if derivative:
+        abar = coulomb * dt[:, :, None] * cvec[None, None, :]
+        mbar_plus = 0.5 * coulomb * np.outer(rho, rho)
+        for d in ds:
+            daq = np.einsum("ml,qls,sn->qmn", d, aq, d, optimize=True)
+            abar += exchange * np.einsum("pq,qmn->mnp", mf.pinv, daq, optimize=True)
+            mbar_plus += 0.5 * exchange * np.einsum("pmn,qmn->pq", aq, daq, optimize=True)
+        mbar = metric_response(mf, mbar_plus, relative_threshold)
+        out["gradient"] = grad3c(orb, aux, xyz, abar) + grad2c(aux, xyz, mbar)
+    return out

@@ -19,8 +19,8 @@ from vibeqc_b200.plan import make_molecule
 def _batch(n=2, seed=0):
     mols = [make_molecule(geometry.water_cluster(k + 1, seed + k), "def2-svp", "cc-pvdz-jkfit")
             for k in range(n)]
-    calc = SimpleNamespace(basis="def2-svp", auxiliary_basis="cc-pvdz-jkfit", spherical=True,
-                           device=torch.device("cpu"))
+    calc = SimpleNamespace(method="rhf", basis="def2-svp", auxiliary_basis="cc-pvdz-jkfit",
+                           spherical=True, device=torch.device("cpu"))
     b = SimpleNamespace(_molecules=mols, _calc=calc, size=n, _warm=[None] * n,
                         _warm_origin=[None] * n, _source_coordinates=[None] * n)
     return b

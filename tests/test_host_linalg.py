@@ -87,6 +87,78 @@ def test_gradient_weights_match_dense_formulas(n, o, x, upper, monkeypatch):
         assert torch.allclose(mbar[m], ref_mbar, rtol=0, atol=1e-11 * ref_mbar.abs().max().item())
 
 
+def test_unrestricted_gradient_weights_match_dense_formulas(monkeypatch):
+    """Two spin channels c_s = C_s / sqrt(2): Abar = D_t (x) cvec - sum_s C_s Gamma_s C_s^T,
+    Mbar = -cc^T/2 + 1/2 sum_s Gamma_s Gamma_s^T (Gamma_s from the unscaled C_s)."""
+    from vibeqc_b200 import gradient as gr
+
+    monkeypatch.setattr(gr, "WEIGHT_ROW_BLOCK", 8)
+    monkeypatch.setattr(gr, "SYM_BLOCK", 64)
+    g = torch.Generator().manual_seed(11)
+    nb, n, o, x = 2, 17, 4, 60
+    cs = [torch.randn(nb, n, o, dtype=torch.float64, generator=g) for _ in range(2)]
+    cs[1][:, :, 3] = 0.0  # beta padded with a zero column
+    bfull = torch.randn(nb, n, n, x, dtype=torch.float64, generator=g)
+    bfull = 0.5 * (bfull + bfull.transpose(1, 2))
+    w = torch.triu(torch.randn(nb, x, x, dtype=torch.float64, generator=g))
+    ds = [c @ c.transpose(1, 2) for c in cs]
+    dt = ds[0] + ds[1]
+    rho = torch.einsum("bmnq,bmn->bq", bfull, dt)
+    abar = torch.empty(nb, n * (n + 1) // 2, x, dtype=torch.float64)
+    mbar = torch.empty(nb, x, x, dtype=torch.float64)
+    for ch, c in enumerate(cs):
+        ct = c / 2 ** 0.5
+        u = torch.einsum("bmnq,bni->bmiq", bfull, ct)
+        gr.chunk_weights(ct, dt, rho, u, w, True, abar, mbar, k_scale=2.0, coulomb=ch == 0)
+    mu, nu = torch.tril_indices(n, n)
+    for m in range(nb):
+        cvec = w[m] @ rho[m]
+        full = dt[m][:, :, None] * cvec
+        ref_mbar = -0.5 * torch.outer(cvec, cvec)
+        for c in cs:
+            bij = torch.einsum("mi,mnq,nj->qij", c[m], bfull[m], c[m])
+            gam = (w[m] @ bij.reshape(x, o * o)).view(x, o, o)
+            full = full - torch.einsum("mi,nj,pij->mnp", c[m], c[m], gam)
+            ref_mbar = ref_mbar + 0.5 * gam.reshape(x, -1) @ gam.reshape(x, -1).T
+        ref_abar = full[mu, nu]
+        assert torch.allclose(abar[m], ref_abar, rtol=0, atol=1e-11 * ref_abar.abs().max().item())
+        assert torch.allclose(mbar[m], ref_mbar, rtol=0, atol=1e-11 * ref_mbar.abs().max().item())
+
+
+def test_uhf_post_block_matches_plain_restatement():
+    from vibeqc_b200 import uhf
+
+    g = torch.Generator().manual_seed(5)
+    nb, n, x, hist = 2, 7, 4, 3
+
+    def sym(*shape):
+        a = torch.randn(*shape, dtype=torch.float64, generator=g)
+        return 0.5 * (a + a.transpose(-1, -2))
+
+    h, s = sym(nb, n, n), sym(nb, n, n) + 4 * torch.eye(n, dtype=torch.float64)
+    xo = torch.randn(nb, n, n, dtype=torch.float64, generator=g)
+    enuc = torch.randn(nb, dtype=torch.float64, generator=g)
+    post = uhf._UHFPost(nb, n, x, hist, False, "cpu")
+    post.load(h, s, xo, enuc)
+    errs, focks = [], []
+    for it in range(5):
+        j, ka, kb, da, db = (sym(nb, n, n) for _ in range(5))
+        f, energy, cmax, f_ext = post.run(j, ka, kb, da, db)
+        fa, fb = h + j - ka, h + j - kb
+        e_ref = (0.5 * ((da + db) * h).sum(dim=(1, 2)) + 0.5 * (da * fa).sum(dim=(1, 2))
+                 + 0.5 * (db * fb).sum(dim=(1, 2)) + enuc)
+        assert torch.allclose(energy, e_ref, atol=1e-12)
+        res = [fs @ ds @ s - s @ ds @ fs for fs, ds in ((fa, da), (fb, db))]
+        assert torch.allclose(cmax, torch.maximum(res[0].abs().amax(dim=(1, 2)),
+                                                  res[1].abs().amax(dim=(1, 2))))
+        errs.append(torch.cat([xo.transpose(1, 2) @ r @ xo for r in res], dim=1))
+        focks.append(torch.cat([fa, fb], dim=1))
+        errs, focks = errs[-hist:], focks[-hist:]
+        ref = _reference_diis(errs, focks) if len(errs) > 1 else focks[-1]
+        got = torch.cat([f_ext[0], f_ext[1]], dim=1)
+        assert torch.allclose(got, ref, atol=1e-9 * ref.abs().max().item())
+
+
 def _reference_diis(errs, focks):
     """Pulay extrapolation over the given vectors (plain restatement)."""
     nh = len(errs)

@@ -5,9 +5,10 @@ Same constructor keywords, methods and result records as the reference's
 (``prepare_batch``), ``:2128`` (``singlepoint``) and
 ``python/generativeqc/batch.py:58-121,799`` (``BatchItemResult``,
 ``BatchResult``, ``PreparedBatch.execute``).  Units are Bohr and Hartree;
-forces are -dE/dR.  Only ``method="rhf"`` with ``density_fitting="cuda"``
-(or ``"auto"``/``True``) on ``device="cuda"`` is served here; any other
-combination raises ``NotImplementedError`` naming the unsupported option.
+forces are -dE/dR.  Only ``method="rhf"`` (closed-shell singlets) or ``method="uhf"`` (any
+multiplicity) with ``density_fitting="cuda"`` (or ``"auto"``/``True``) on
+``device="cuda"`` is served here; any other combination raises
+``NotImplementedError`` naming the unsupported option.
 """
 
 from __future__ import annotations
@@ -20,9 +21,10 @@ import numpy as np
 import torch
 
 from . import _lib, tuning
-from .gradient import df_rhf_gradient
+from .gradient import df_rhf_gradient, df_uhf_gradient
 from .plan import make_molecule
 from .scf import Chunk, compute_integrals, run_scf
+from .uhf import run_scf_uhf
 
 STATUS_SUCCESS = 0
 STATUS_INVALID_ARGUMENT = 1
@@ -119,8 +121,8 @@ class Calculator:
     ) -> None:
         if unsupported:
             raise NotImplementedError(f"options outside the DF-RHF CUDA path: {sorted(unsupported)}")
-        if str(method).lower() != "rhf":
-            raise NotImplementedError("only method='rhf' is served by this engine")
+        if str(method).lower() not in ("rhf", "uhf"):
+            raise NotImplementedError("only method='rhf' or 'uhf' is served by this engine")
         if density_fitting not in ("cuda", "auto", True):
             raise NotImplementedError("this engine serves density_fitting='cuda' (or 'auto'/True)")
         if device != "cuda":
@@ -138,7 +140,7 @@ class Calculator:
         if not torch.cuda.is_available():
             raise RuntimeError("no CUDA device is visible")
         _lib.lib()  # fail loudly if the native library is missing
-        self.method = "rhf"
+        self.method = str(method).lower()
         self.basis = basis
         self.auxiliary_basis = auxiliary_basis
         self.device = torch.device("cuda", device_id)
@@ -197,24 +199,27 @@ class PreparedBatch:
         self._molecules = []
         for atoms, q, m in zip(systems, charges, mults):
             mol = make_molecule(atoms, calculator.basis, calculator.auxiliary_basis, q, m)
-            if m != 1 or mol.nelectron % 2:
+            if calculator.method == "rhf" and (m != 1 or mol.nelectron % 2):
                 raise NotImplementedError("RHF needs a closed-shell singlet (multiplicity 1, even electrons)")
             self._molecules.append(mol)
-        # homogeneous chunks: identical (nao, naux, nocc), input order kept inside a chunk
+        self._unrestricted = calculator.method == "uhf"
+        # homogeneous chunks: identical (nao, naux, n_alpha, n_beta), input order
+        # kept inside a chunk
         groups: dict = {}
         from . import basis as bas
 
         for i, mol in enumerate(self._molecules):
             key = (bas.count_functions(mol.orbital_shells, calculator.spherical),
-                   bas.count_functions(mol.aux_shells, calculator.spherical), mol.nocc)
+                   bas.count_functions(mol.aux_shells, calculator.spherical), mol.nalpha,
+                   mol.nbeta)
             groups.setdefault(key, []).append(i)
         budget = calculator.memory_budget_bytes
         if budget <= 0:
             budget = int(0.6 * torch.cuda.get_device_properties(calculator.device).total_memory)
         self._chunks = []
-        for (nao, naux, nocc), idx in sorted(groups.items()):
+        for (nao, naux, nocc, _nbeta), idx in sorted(groups.items()):
             prec = chunk_precision(calculator.precision, nao, nocc)
-            per_mol = _device_bytes_per_molecule(nao, naux, prec)
+            per_mol = _device_bytes_per_molecule(nao, naux, prec, self._unrestricted)
             limit = max(1, budget // per_mol)
             for s in range(0, len(idx), limit):
                 part = idx[s:s + limit]
@@ -279,7 +284,8 @@ class PreparedBatch:
             return None, None
         dev = self._calc.device
         n = chunk.nao
-        dens = torch.zeros(chunk.nb, n, n, dtype=torch.float64, device=dev)
+        shape = (chunk.nb, 2, n, n) if self._unrestricted else (chunk.nb, n, n)
+        dens = torch.zeros(*shape, dtype=torch.float64, device=dev)
         mask = torch.zeros(chunk.nb, dtype=torch.bool, device=dev)
         for j, i in enumerate(chunk.indices):
             if self._warm[i] is not None:
@@ -317,18 +323,23 @@ class PreparedBatch:
         ints = compute_integrals(chunk.plan, xyz)
         warm_density, warm_mask = self._chunk_warm(chunk)
         schedule = tuning.active_table().lookup(chunk.nao, chunk.naux, chunk.nocc)
-        out = run_scf(chunk, ints, xyz, precision=chunk.precision, schedule=schedule,
+        driver = run_scf_uhf if self._unrestricted else run_scf
+        out = driver(chunk, ints, xyz, precision=chunk.precision, schedule=schedule,
                       max_iterations=calc.max_iterations,
                       energy_tolerance=calc.energy_tolerance,
                       density_tolerance=calc.density_tolerance,
                       diis_history=calc.diis_history,
                       relative_threshold=calc.relative_threshold,
                       warm_density=warm_density, warm_mask=warm_mask)
-        grad = df_rhf_gradient(chunk, ints, out, xyz) if want_forces else None
+        gradient = df_uhf_gradient if self._unrestricted else df_rhf_gradient
+        grad = gradient(chunk, ints, out, xyz) if want_forces else None
         # keep only per-molecule results; the chunk's B tensor and factors go
         mf = out.pop("metric")
         slim = {k: out[k] for k in ("energy", "converged", "iterations", "energy_change",
                                     "density_rms", "density", "warm_used", "warm_fallback")}
+        if self._unrestricted:
+            # the retained warm-start state is the pair of spin densities
+            slim["density"] = torch.stack(out["spin_densities"], dim=1)
         slim["metric_rank"] = mf.rank
         slim["metric_condition"] = mf.condition
         slim["metric_kind"] = mf.kind
@@ -492,7 +503,8 @@ def chunk_precision(requested: str, nao: int, nocc: int) -> str:
     return "mixed"
 
 
-def _device_bytes_per_molecule(nao: int, naux: int, precision: str) -> int:
+def _device_bytes_per_molecule(nao: int, naux: int, precision: str,
+                               unrestricted: bool = False) -> int:
     """Peak device bytes one molecule holds during a chunk (integrals to gradient)."""
     p = nao * (nao + 1) // 2
     # fp64: full FP64 B (16) + packed A during whitening / packed Abar (8) + K temporaries;
@@ -500,6 +512,8 @@ def _device_bytes_per_molecule(nao: int, naux: int, precision: str) -> int:
     # N*o*X elements (~2o/N * 24 per packed element) + anchor temporaries;
     # the FP32 buffers are released before the packed Abar (8) is formed
     per_px = 30 if precision == "fp64" else 40
+    if unrestricted:
+        per_px += 8  # a second spin channel's anchor and U buffers
     return int(per_px * p * naux + 64 * nao * nao)
 
 

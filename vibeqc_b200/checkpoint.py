@@ -62,7 +62,7 @@ def _item_identity(batch, i: int) -> dict:
 
 def _model(batch) -> dict:
     calc = batch._calc
-    return {"method": "rhf", "basis": str(calc.basis).lower(),
+    return {"method": calc.method, "basis": str(calc.basis).lower(),
             "auxiliary_basis": str(calc.auxiliary_basis).lower(),
             "representation": "spherical" if calc.spherical else "cartesian"}
 
@@ -172,7 +172,8 @@ def load_checkpoint(batch, path, *, allow_warm: bool = False, strict: bool = Tru
             dens = arrays.get(f"density/{i}")
             xyz = arrays.get(f"coordinates/{i}")
             n = want["nao"]
-            if dens is None or xyz is None or dens.shape != (n, n) or not np.isfinite(dens).all():
+            shape = (2, n, n) if batch._calc.method == "uhf" else (n, n)
+            if dens is None or xyz is None or dens.shape != shape or not np.isfinite(dens).all():
                 reason = "missing or invalid density"
             elif not allow_warm and not np.array_equal(xyz, batch._molecules[i].coordinates):
                 reason = "coordinates differ (pass allow_warm=True for a changed geometry)"

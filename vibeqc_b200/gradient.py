@@ -76,7 +76,8 @@ def _block_rows(n: int, m0: int, m1: int, device) -> torch.Tensor:
 
 def chunk_weights(c: torch.Tensor, dens: torch.Tensor, rho: torch.Tensor, u: torch.Tensor,
                   w: torch.Tensor, upper: bool, abar: torch.Tensor | None = None,
-                  mbar: torch.Tensor | None = None):
+                  mbar: torch.Tensor | None = None, k_scale: float = 1.0,
+                  coulomb: bool = True):
     """Packed Abar (b, N(N+1)/2, X) and Mbar (b, X, X) for b molecules at once.
 
     c (b, N, o) occupied factors (D = 2 c c^T), rho (b, X) whitened fitted
@@ -86,9 +87,13 @@ def chunk_weights(c: torch.Tensor, dens: torch.Tensor, rho: torch.Tensor, u: tor
     over nu < m1 followed by the rank-one D (x) c term, so the full N*N*X
     tensor is never formed.  Every product is a batched GEMM over the b
     molecules (a handful of launches per chunk instead of per molecule).
+
+    ``k_scale`` multiplies the exchange terms (1 for the restricted energy;
+    2 for one spin channel of an unrestricted one, whose factor is
+    C_s / sqrt(2)).  With ``coulomb`` False only the exchange terms of c are
+    added to the given ``abar`` and ``mbar`` (a further spin channel).
     """
     b, n, o, x = u.shape
-    cvec = torch.bmm(w, rho[:, :, None])[:, :, 0]  # raw-basis fitting coefficients Minv rho
     # C^T B_Q C: [i][j][Q] from one GEMM, then [Q][i][j]
     bij = torch.bmm(c.transpose(1, 2), u.reshape(b, n, o * x)).view(b, o, o, x)
     bij = bij.permute(0, 3, 1, 2).reshape(b, x, o * o)
@@ -102,16 +107,29 @@ def chunk_weights(c: torch.Tensor, dens: torch.Tensor, rho: torch.Tensor, u: tor
         abar = torch.empty(b, n * (n + 1) // 2, x, dtype=u.dtype, device=u.device)
     if mbar is None:
         mbar = torch.empty(b, x, x, dtype=u.dtype, device=u.device)
-    mu_all, nu_all = torch.tril_indices(n, n, device=u.device)
-    dpairs = dens[:, mu_all, nu_all]
+    if coulomb:
+        cvec = torch.bmm(w, rho[:, :, None])[:, :, 0]  # raw-basis fitting coefficients Minv rho
+        mu_all, nu_all = torch.tril_indices(n, n, device=u.device)
+        dpairs = dens[:, mu_all, nu_all]
     for m0 in range(0, n, WEIGHT_ROW_BLOCK):
         m1 = min(n, m0 + WEIGHT_ROW_BLOCK)
         blk = torch.bmm(c[:, m0:m1], t1[:, :, : m1 * x]).view(b, -1, x)  # (mu) x (nu < m1, P)
         p0, p1 = m0 * (m0 + 1) // 2, m1 * (m1 + 1) // 2
-        abar[:, p0:p1] = torch.baddbmm(blk[:, _block_rows(n, m0, m1, u.device)],
-                                       dpairs[:, p0:p1, None], cvec[:, None, :], beta=-2.0, alpha=1.0)
-    _sym_gram(gam, mbar)
-    mbar.baddbmm_(cvec[:, :, None], cvec[:, None, :], alpha=-0.5)
+        rows = blk[:, _block_rows(n, m0, m1, u.device)]
+        if coulomb:
+            abar[:, p0:p1] = torch.baddbmm(rows, dpairs[:, p0:p1, None], cvec[:, None, :],
+                                           beta=-2.0 * k_scale, alpha=1.0)
+        else:
+            abar[:, p0:p1].add_(rows, alpha=-2.0 * k_scale)
+    if coulomb:
+        _sym_gram(gam, mbar)
+        if k_scale != 1.0:
+            mbar.mul_(k_scale)
+        mbar.baddbmm_(cvec[:, :, None], cvec[:, None, :], alpha=-0.5)
+    else:
+        g2 = torch.empty_like(mbar)
+        _sym_gram(gam, g2)
+        mbar.add_(g2, alpha=k_scale)
     return abar, mbar
 
 
@@ -145,59 +163,89 @@ def spectral_metric_adjoint(lam: torch.Tensor, vec: torch.Tensor, keep: torch.Te
     return vec @ ((vec.transpose(0, 1) @ mbar_plus @ vec) * gam) @ vec.transpose(0, 1)
 
 
-def _raw_mbar_plus(a_raw_packed: torch.Tensor, c: torch.Tensor, n: int) -> torch.Tensor:
-    """Mbar+ = rho rho^T / 2 - sum_ij A_ij A_ij^T in the raw auxiliary basis (one molecule).
+def _raw_mbar_plus(a_raw_packed: torch.Tensor, channels, n: int) -> torch.Tensor:
+    """Mbar+ = rho rho^T / 2 - sum_(c, k) k sum_ij A_ij A_ij^T in the raw auxiliary basis.
 
-    A_ij[P] = sum_{mu nu} C[mu i] C[nu j] (mu nu|P), rho = sum D A = 2 sum_i A_ii.
+    ``channels``: (c (N, o), k) pairs for one molecule, D = 2 c c^T per channel
+    (k = 1 restricted; k = 2 per spin channel C_s / sqrt(2) of an unrestricted
+    density); A_ij[P] = sum_{mu nu} c[mu i] c[nu j] (mu nu|P) and
+    rho = sum over channels of 2 sum_i A_ii.
     """
     x = a_raw_packed.shape[1]
-    o = c.shape[1]
     a_full = a_raw_packed[unpack_index(n, a_raw_packed.device)]  # (N*N, X)
-    ui = (c.transpose(0, 1) @ a_full.view(n, n * x)).view(o, n, x)  # [i][nu][P]
-    del a_full
-    aij = torch.einsum("nj,inp->ijp", c, ui).reshape(o * o, x)
-    rho = 2.0 * aij.view(o, o, x).diagonal(dim1=0, dim2=1).sum(dim=1)
-    return 0.5 * torch.outer(rho, rho) - aij.transpose(0, 1) @ aij
+    rho = torch.zeros(x, dtype=a_full.dtype, device=a_full.device)
+    quad = torch.zeros(x, x, dtype=a_full.dtype, device=a_full.device)
+    for c, k in channels:
+        o = c.shape[1]
+        ui = (c.transpose(0, 1) @ a_full.view(n, n * x)).view(o, n, x)  # [i][nu][P]
+        aij = torch.einsum("nj,inp->ijp", c, ui).reshape(o * o, x)
+        rho += 2.0 * aij.view(o, o, x).diagonal(dim1=0, dim2=1).sum(dim=1)
+        quad += k * (aij.transpose(0, 1) @ aij)
+    return 0.5 * torch.outer(rho, rho) - quad
 
 
 def df_rhf_gradient(chunk, ints, scf_out: dict, xyz: torch.Tensor) -> torch.Tensor:
     """Positive energy gradient, (natom_total_of_chunk, 3)."""
-    plan = chunk.plan
-    nb, n, x, o = chunk.nb, chunk.nao, chunk.naux, chunk.nocc
-    dev = xyz.device
-    mf = scf_out["metric"]
-    truncated = [m for m in range(nb) if mf.rank[m] < x]
     dens = scf_out["density"]
     c = scf_out["orbitals"]  # AO occupied factor, dens = 2 c c^T
-    f = scf_out["fock"]
-    jk = scf_out["jk"]
     # energy-weighted density of the converged closed shell: W = D F D / 2
-    wdens = 0.5 * dens @ f @ dens
+    wdens = 0.5 * dens @ scf_out["fock"] @ dens
+    if scf_out.get("exact_half") is not None:
+        half = scf_out["exact_half"]  # FP64 U = B C already formed for the energy
+    else:
+        half = scf_out["jk"].half_transform(c)  # fitted density and U = B C
+    return _df_gradient(chunk, scf_out, xyz, dens, wdens, [(c, half, 1.0)])
 
+
+def df_uhf_gradient(chunk, ints, scf_out: dict, xyz: torch.Tensor) -> torch.Tensor:
+    """Positive unrestricted energy gradient, (natom_total_of_chunk, 3).
+
+    Reverse weights as the reference's unrestricted weighted gradient
+    (``src/scf/density_fitting.cpp:919-944``): Coulomb on D_a + D_b, exchange
+    per spin density; energy-weighted density W = sum_s D_s F_s D_s.
+    """
+    ds = scf_out["spin_densities"]
+    cs = scf_out["orbitals"]  # channel factors C_s / sqrt(2), D_s = 2 c_s c_s^T
+    dens = ds[0] + ds[1]
+    wdens = sum(d @ f @ d for d, f in zip(ds, scf_out["fock"]))
+    halves = scf_out.get("exact_half")
+    if halves is None:
+        halves = [scf_out["jk"].half_transform(c) for c in cs]
+    return _df_gradient(chunk, scf_out, xyz, dens, wdens,
+                        [(c, half, 2.0) for c, half in zip(cs, halves)])
+
+
+def _df_gradient(chunk, scf_out, xyz, dens, wdens, channels) -> torch.Tensor:
+    """Weights from ``channels`` [(c, (rho, U = B c), k_scale)], then the derivative contractions."""
+    plan = chunk.plan
+    nb, n, x = chunk.nb, chunk.nao, chunk.naux
+    dev = xyz.device
+    mf = scf_out["metric"]
+    jk = scf_out["jk"]
+    truncated = [m for m in range(nb) if mf.rank[m] < x]
+    o = channels[0][0].shape[2]
     wctx = TIMER.stage("grad_weights")
     wctx.__enter__()
-    if scf_out.get("exact_half") is not None:
-        rho_all, u_all = scf_out["exact_half"]  # FP64 U = B C already formed for the energy
-    else:
-        rho_all, u_all = jk.half_transform(c)  # fitted density and U = B C
+    rho_all = sum(half[0] for _, half, _ in channels)
     abar = torch.empty(nb, n * (n + 1) // 2, x, dtype=torch.float64, device=dev)
     mbar = torch.empty(nb, x, x, dtype=torch.float64, device=dev)
     tri = mf.kind == "cholesky"
     grp = max(1, WEIGHT_GROUP_BYTES // max(1, 8 * n * o * x))
     for g0 in range(0, nb, grp):  # groups of molecules: bounded temporaries
         g1 = min(nb, g0 + grp)
-        chunk_weights(c[g0:g1], dens[g0:g1], rho_all[g0:g1], u_all[g0:g1], mf.inv_sqrt[g0:g1], tri,
-                      abar[g0:g1], mbar[g0:g1])
+        for ch, (c, (_, u_all), k) in enumerate(channels):
+            chunk_weights(c[g0:g1], dens[g0:g1], rho_all[g0:g1], u_all[g0:g1], mf.inv_sqrt[g0:g1],
+                          tri, abar[g0:g1], mbar[g0:g1], k_scale=k, coulomb=ch == 0)
     if truncated:
         # the whitened tensor is no longer needed: recompute the raw one for
         # the spectral response of the truncated metrics
-        del u_all
+        channels = [(c, None, k) for c, _, k in channels]
         jk.release_all()
         from .scf import compute_integrals
 
         a_raw = compute_integrals(plan, xyz).a_packed
         for m in truncated:
-            mbp = _raw_mbar_plus(a_raw[m], c[m], n)
+            mbp = _raw_mbar_plus(a_raw[m], [(c[m], k) for c, _, k in channels], n)
             mbar[m] = spectral_metric_adjoint(mf.eigenvalues[m], mf.eigenvectors[m], mf.keep[m], mbp,
                                               scf_out["relative_threshold"])
         del a_raw

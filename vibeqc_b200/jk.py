@@ -52,12 +52,14 @@ class FP64Builder:
         self.b = b_packed[:, idx, :].contiguous()  # (nb, N*N, X)
         self.nbuild = 0
 
-    def build(self, d: torch.Tensor, c_occ: torch.Tensor):
+    def build(self, d: torch.Tensor, c_occ: torch.Tensor, with_j: bool = True):
         nb, n, x, o = d.shape[0], self.n, self.x, self.nocc
         b = self.b
-        with TIMER.stage("J_fp64"):
-            rho = torch.bmm(d.reshape(nb, 1, n * n), b)  # (nb, 1, X)
-            j = torch.bmm(b, rho.transpose(1, 2)).reshape(nb, n, n)
+        j = None
+        if with_j:
+            with TIMER.stage("J_fp64"):
+                rho = torch.bmm(d.reshape(nb, 1, n * n), b)  # (nb, 1, X)
+                j = torch.bmm(b, rho.transpose(1, 2)).reshape(nb, n, n)
         with TIMER.stage("K_fp64"):
             # U[i][mu][Q] = sum_nu C[nu, i] B[nu, mu Q] (B symmetric in mu, nu),
             # K = 2 sum_i U_i U_i^T
@@ -67,8 +69,8 @@ class FP64Builder:
         self.nbuild += 1
         return j, k
 
-    def build_exact(self, d: torch.Tensor, c_occ: torch.Tensor):
-        return self.build(d, c_occ)
+    def build_exact(self, d: torch.Tensor, c_occ: torch.Tensor, with_j: bool = True):
+        return self.build(d, c_occ, with_j)
 
     def half_transform(self, c_occ: torch.Tensor):
         """(rho_whitened (nb, X), U (nb, N, o, X)) for D = 2 C C^T."""
@@ -129,6 +131,8 @@ class MixedBuilder:
         # than gathering from the packed rows)
         self.b64 = b_packed[:, unpack_index(n, dev), :].contiguous()  # (nb, N*N, X)
         self.err = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.v_hi = self.v_lo = None
+        self._anc: dict = {}  # anchor state per channel (spin)
         self.nbuild = 0
 
     def _check(self):
@@ -155,18 +159,21 @@ class MixedBuilder:
                            self.ldq, self.u_hi.data_ptr(), self.u_lo.data_ptr(),
                            0 if rho is None else rho.data_ptr(), self.err.data_ptr(), self.st)
 
-    def build(self, d: torch.Tensor, c_occ: torch.Tensor):
+    def build(self, d: torch.Tensor, c_occ: torch.Tensor, with_j: bool = True):
         nb, n = self.nb, self.n
         self._half(c_occ)
-        j = torch.empty(nb, n, n, dtype=torch.float64, device=d.device)
-        with TIMER.stage("J_fp32"):
-            # fitted density from the FP32 B with FP64 accumulation (no
-            # tensor-core accumulation error in J), then J = B rho
-            dd = d.contiguous()
-            self._lib.call("vqc_fitted_density_fp32", self.b.data_ptr(), dd.data_ptr(), nb, n,
-                           self.ld, self.x, self.rho_part.data_ptr(), self.rho.data_ptr(), self.st)
-            self._lib.call("vqc_coulomb_fp32", self.b.data_ptr(), self.rho.data_ptr(), nb, n,
-                           self.ld, self.x, j.data_ptr(), self.st)
+        j = None
+        if with_j:
+            j = torch.empty(nb, n, n, dtype=torch.float64, device=d.device)
+            with TIMER.stage("J_fp32"):
+                # fitted density from the FP32 B with FP64 accumulation (no
+                # tensor-core accumulation error in J), then J = B rho
+                dd = d.contiguous()
+                self._lib.call("vqc_fitted_density_fp32", self.b.data_ptr(), dd.data_ptr(), nb, n,
+                               self.ld, self.x, self.rho_part.data_ptr(), self.rho.data_ptr(),
+                               self.st)
+                self._lib.call("vqc_coulomb_fp32", self.b.data_ptr(), self.rho.data_ptr(), nb, n,
+                               self.ld, self.x, j.data_ptr(), self.st)
         k = torch.zeros(nb, n, n, dtype=torch.float64, device=d.device)
         COUNTERS["k_flops"] += nb * self.x * self.nocc * n * (n + 1)
         with TIMER.stage("K_gram_tc"):
@@ -203,41 +210,51 @@ class MixedBuilder:
     # so their split-precision error scales with |D - D0| instead of |D|, and
     # the converged operators are FP64-accurate.
 
-    def anchor(self, d: torch.Tensor, c_occ: torch.Tensor):
+    def anchor(self, d: torch.Tensor, c_occ: torch.Tensor, channel: int = 0, with_j: bool = True):
+        """FP64 J/K at D0 = 2 C0 C0^T; later increments of ``channel`` are about it.
+
+        Each channel (one per spin of an unrestricted SCF) keeps its own anchor;
+        with ``with_j`` False the Coulomb matrix is not formed (returned as None).
+        """
         nb, n, x, o = self.nb, self.n, self.x, self.nocc
         with TIMER.stage("anchor_fp64"):
             rho0, u0 = fp64_half(self.b64, c_occ, n, x)  # u0 (nb, N, o, X)
             uf = u0.view(nb, n, o * x)
             k0 = 2.0 * torch.bmm(uf, uf.transpose(1, 2))
-            j0 = torch.bmm(self.b64, rho0[:, :, None]).view(nb, n, n)
-        self.c0 = c_occ.clone()
-        self.rho0, self.j0, self.k0, self.u0 = rho0, j0, k0, u0
-        if not hasattr(self, "v_hi"):
+            j0 = torch.bmm(self.b64, rho0[:, :, None]).view(nb, n, n) if with_j else None
+        self._anc[channel] = {"c0": c_occ.clone(), "rho0": rho0, "j0": j0, "k0": k0, "u0": u0}
+        if self.v_hi is None:
             self.v_hi = torch.empty_like(self.u_hi)
             self.v_lo = torch.empty_like(self.u_hi)
         self.nbuild += 1
         return j0, k0, rho0
 
-    def _increment(self, c_occ: torch.Tensor):
+    def _increment(self, c_occ: torch.Tensor, channel: int):
         """dU = B (C - C0) into u_hi/u_lo; returns rho - rho0."""
-        dc = c_occ - self.c0
+        c0 = self._anc[channel]["c0"]
+        dc = c_occ - c0
         drho = torch.zeros(self.nb, self.x, dtype=torch.float64, device=c_occ.device)
-        self._half(dc, cvec=self.c0 + 0.5 * dc, rho=drho)  # drho = 2 sum (C0 + dC/2) dU
+        self._half(dc, cvec=c0 + 0.5 * dc, rho=drho)  # drho = 2 sum (C0 + dC/2) dU
         return 2.0 * drho
 
-    def build_incremental(self, d: torch.Tensor, c_occ: torch.Tensor):
+    def build_incremental(self, d: torch.Tensor, c_occ: torch.Tensor, channel: int = 0,
+                          with_j: bool = True):
         nb, n, x, o = self.nb, self.n, self.x, self.nocc
-        drho = self._increment(c_occ)
-        dj = torch.empty(nb, n, n, dtype=torch.float64, device=d.device)
-        with TIMER.stage("J_fp32"):
-            self._lib.call("vqc_coulomb_fp32", self.b.data_ptr(), drho.data_ptr(), nb, n,
-                           self.ld, x, dj.data_ptr(), self.st)
+        anc = self._anc[channel]
+        drho = self._increment(c_occ, channel)
+        j = None
+        if with_j:
+            dj = torch.empty(nb, n, n, dtype=torch.float64, device=d.device)
+            with TIMER.stage("J_fp32"):
+                self._lib.call("vqc_coulomb_fp32", self.b.data_ptr(), drho.data_ptr(), nb, n,
+                               self.ld, x, dj.data_ptr(), self.st)
+            j = anc["j0"] + dj
         COUNTERS["k_flops"] += 2 * nb * x * o * n * (n + 1)  # V dU^T + dU V^T
         with TIMER.stage("K_gram_tc"):
-            self._lib.call("vqc_anchor_combine", self.u0.data_ptr(), self.u_hi.data_ptr(),
+            self._lib.call("vqc_anchor_combine", anc["u0"].data_ptr(), self.u_hi.data_ptr(),
                            self.u_lo.data_ptr(), self.v_hi.data_ptr(), self.v_lo.data_ptr(),
                            nb * n * o, x, self.ldq, 0.5, 0, self.st)
-            kh = 0.5 * self.k0
+            kh = 0.5 * anc["k0"]
             self._lib.call("vqc_tc_gram_sym2", self.v_hi.data_ptr(), self.v_lo.data_ptr(),
                            self.u_hi.data_ptr(), self.u_lo.data_ptr(), nb, n, o * self.ldq,
                            kh.data_ptr(), self.err.data_ptr(), self.st)
@@ -245,21 +262,22 @@ class MixedBuilder:
         self._check()
         # K = K0 + 2 (V dU^T + dU V^T) = K0 + (kh - K0/2) + (kh - K0/2)^T: the
         # diagonal tiles' FP32 accumulation order leaves a tiny asymmetry
-        return self.j0 + dj, kh + kh.transpose(1, 2), self.rho0 + drho
+        return j, kh + kh.transpose(1, 2), anc["rho0"] + drho
 
-    def anchored_half(self, c_occ: torch.Tensor):
+    def anchored_half(self, c_occ: torch.Tensor, channel: int = 0):
         """(rho, U = U0 + B (C - C0)) at the final orbitals, FP64 (nb, N, o, X).
 
-        Consumes the anchor: U0 is updated in place.
+        Consumes the channel's anchor: U0 is updated in place.
         """
         nb, n, x, o = self.nb, self.n, self.x, self.nocc
-        drho = self._increment(c_occ)
-        self._lib.call("vqc_anchor_combine", self.u0.data_ptr(), self.u_hi.data_ptr(),
+        anc = self._anc[channel]
+        drho = self._increment(c_occ, channel)
+        self._lib.call("vqc_anchor_combine", anc["u0"].data_ptr(), self.u_hi.data_ptr(),
                        self.u_lo.data_ptr(), 0, 0, nb * n * o, x, self.ldq, 1.0, 1, self.st)
         self._check()
-        u = self.u0
-        self.u0 = None
-        return self.rho0 + drho, u
+        u = anc["u0"]
+        anc["u0"] = None
+        return anc["rho0"] + drho, u
 
 
 def make_builder(precision: str, b_packed: torch.Tensor, n: int, x: int, nocc: int):

@@ -37,7 +37,18 @@ class MoleculeSpec:
 
     @property
     def nocc(self) -> int:
-        return self.nelectron // 2
+        """Doubly occupied orbitals (restricted) or alpha electrons (unrestricted)."""
+        if self.multiplicity == 1:
+            return self.nelectron // 2
+        return self.nalpha
+
+    @property
+    def nalpha(self) -> int:
+        return (self.nelectron + self.multiplicity - 1) // 2
+
+    @property
+    def nbeta(self) -> int:
+        return self.nelectron - self.nalpha
 
 
 def make_molecule(atoms, basis, auxiliary_basis, charge: int = 0, multiplicity: int = 1) -> MoleculeSpec:
@@ -51,7 +62,11 @@ def make_molecule(atoms, basis, auxiliary_basis, charge: int = 0, multiplicity: 
     for s in orb + aux:
         if s.angular_momentum > 3:
             raise ValueError("shells above f are not supported by the CUDA kernels")
-    return MoleculeSpec(z, xyz, orb, aux, charge, multiplicity)
+    nel = int(z.sum()) - int(charge)
+    if int(multiplicity) < 1 or nel < 1 or (nel + int(multiplicity) - 1) % 2 \
+            or int(multiplicity) - 1 > nel:
+        raise ValueError("charge and multiplicity are inconsistent with the electron count")
+    return MoleculeSpec(z, xyz, orb, aux, int(charge), int(multiplicity))
 
 
 @dataclass

@@ -189,6 +189,10 @@ class Chunk:
             if (l_.nao, l_.naux, l_.nocc) != (self.nao, self.naux, self.nocc):
                 raise ValueError("a chunk must be homogeneous in (N, X, n_occ)")
         self.natoms = [len(m.atomic_numbers) for m in molecules]
+        spins = {(m.nalpha, m.nbeta) for m in molecules}
+        if len(spins) != 1:
+            raise ValueError("a chunk must be homogeneous in (n_alpha, n_beta)")
+        self.nalpha, self.nbeta = spins.pop()
         self.precision = "fp64"  # set by the prepared batch from the requested precision
 
     def close(self):
