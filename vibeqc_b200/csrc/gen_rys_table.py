@@ -29,8 +29,8 @@ from pathlib import Path
 import mpmath as mp
 
 NMAX = 7
-DEG = 15          # Chebyshev degree per interval
-H = 1.0           # interval width in T
+DEG = 9           # Chebyshev degree per interval
+H = 0.5           # interval width in T
 DPS = 80
 TOL_ASYM = 1e-15
 
