@@ -210,25 +210,37 @@ def _orthogonalizer(s: torch.Tensor) -> torch.Tensor:
 
 
 SP2_GRAPH_STEPS = 8  # SP2 steps per captured CUDA graph (even: ends in the same buffer)
+SP2_SLICES = 7  # 7-bit slices per operand of the int8 tensor-core X^2 (FP64-accurate products)
 # native kernels launched by graph replays (the library's own launch counter
 # sees only direct launches)
 GRAPH_LAUNCHES = [0]
 
 
 class _SP2Graph:
-    """SP2_GRAPH_STEPS SP2 steps (batched DGEMM + vqc_sp2_update) as one CUDA graph.
+    """SP2_GRAPH_STEPS SP2 steps (X^2 + vqc_sp2_update) as one CUDA graph.
 
     The iterate lives in static buffers; converged molecules are copied
     unchanged by the update kernel, so extra steps are harmless and the host
-    reads the device flags once per replay.
+    reads the device flags once per replay.  ``gemm`` selects how X^2 is
+    formed: "fp64" (batched DGEMM) or "int8" (FP64-accurate products of
+    SP2_SLICES 7-bit slices on the int8 tensor cores, vqc_ozaki_slice_rows +
+    vqc_ozaki_gemm; X is symmetric, so X X^T = X^2, and the sliced product is
+    exactly symmetric because both operands carry the same slices).
     """
 
-    def __init__(self, nb: int, n: int, nocc: int, tol: float, device, steps: int = SP2_GRAPH_STEPS):
+    def __init__(self, nb: int, n: int, nocc: int, tol: float, device, steps: int = SP2_GRAPH_STEPS,
+                 gemm: str = "fp64"):
         self.steps = int(steps)
+        self.gemm = gemm
         self.x = torch.zeros(nb, n, n, dtype=torch.float64, device=device)
         self.x2 = torch.empty_like(self.x)
         self.xn = torch.empty_like(self.x)
         self.done = torch.zeros(nb, dtype=torch.int32, device=device)
+        self.err = torch.zeros(1, dtype=torch.int32, device=device)
+        if gemm == "int8":
+            self.ldk = (n + 15) // 16 * 16
+            self.sl = torch.zeros(nb * SP2_SLICES * n * self.ldk, dtype=torch.int8, device=device)
+            self.ex = torch.zeros(nb * n, dtype=torch.int32, device=device)
         self.args = (nb, n, float(nocc), float(tol))
         self.graph = None
         if os.environ.get("VQC_SP2_GRAPHS", "1") == "0":
@@ -238,24 +250,41 @@ class _SP2Graph:
         with torch.cuda.stream(side):  # warm-up outside capture (cuBLAS handles, workspaces)
             self._steps()
         torch.cuda.current_stream(device).wait_stream(side)
-        self.graph = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(self.graph):
-            self._steps()
+        try:
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph):
+                self._steps()
+            self.graph = graph
+        except Exception:  # a capture the runtime refuses: run the same launches eagerly
+            torch.cuda.synchronize(device)
+            self.graph = None
 
     def run(self):
         """``steps`` steps: one graph replay, or eager launches."""
         if self.graph is not None:
             self.graph.replay()
-            GRAPH_LAUNCHES[0] += self.steps
+            GRAPH_LAUNCHES[0] += self.steps * (3 if self.gemm == "int8" else 1)
         else:
             self._steps()
+
+    def _square(self, x):
+        nb, n = self.args[0], self.args[1]
+        if self.gemm != "int8":
+            torch.bmm(x, x, out=self.x2)
+            return
+        st = torch.cuda.current_stream().cuda_stream
+        _lib.call("vqc_ozaki_slice_rows", x.data_ptr(), nb, n, n, n, n * n, None, SP2_SLICES,
+                  self.sl.data_ptr(), self.ldk, self.ex.data_ptr(), st)
+        _lib.call("vqc_ozaki_gemm", self.sl.data_ptr(), self.ex.data_ptr(), n, self.sl.data_ptr(),
+                  self.ex.data_ptr(), n, n, self.ldk, nb, SP2_SLICES, 0, self.x2.data_ptr(), n, n * n,
+                  self.err.data_ptr(), st)
 
     def _steps(self):
         nb, n, nocc, tol = self.args
         st = torch.cuda.current_stream().cuda_stream
         x, xn = self.x, self.xn
         for _ in range(self.steps):
-            torch.bmm(x, x, out=self.x2)
+            self._square(x)
             _lib.call("vqc_sp2_update", x.data_ptr(), self.x2.data_ptr(), xn.data_ptr(), nb, n,
                       nocc, tol, self.done.data_ptr(), st)
             x, xn = xn, x
@@ -268,7 +297,8 @@ SP2_GRAPH_CACHE_BYTES = 4 << 30  # drop the cache when its buffers would exceed 
 
 
 def purify_sp2(fo: torch.Tensor, nocc: int, max_steps: int = 96, tol: float = 1e-11,
-               graphs: dict | None = None, steps: int = SP2_GRAPH_STEPS) -> torch.Tensor:
+               graphs: dict | None = None, steps: int = SP2_GRAPH_STEPS,
+               gemm: str = "fp64") -> torch.Tensor:
     """Projector onto the lowest ``nocc`` eigenvectors of symmetric ``fo``.
 
     Second-order spectral projection (Niklasson, Phys. Rev. B 66, 155115
@@ -278,7 +308,9 @@ def purify_sp2(fo: torch.Tensor, nocc: int, max_steps: int = 96, tol: float = 1e
     kernel (vqc_sp2_update); convergence flags stay on the device.  Steps run
     in CUDA graphs of SP2_GRAPH_STEPS (cached in ``graphs``, one per shape and
     tolerance), and the flags are read once per graph replay.  ``steps`` (even)
-    is the number of steps per graph (an autotuned schedule choice).
+    is the number of steps per graph and ``gemm`` the X^2 product ("fp64"
+    DGEMM or "int8" sliced tensor-core products), both autotuned schedule
+    choices.
     """
     nb, n, _ = fo.shape
     diag = torch.diagonal(fo, dim1=1, dim2=2)
@@ -286,7 +318,7 @@ def purify_sp2(fo: torch.Tensor, nocc: int, max_steps: int = 96, tol: float = 1e
     emin = (diag - radius).min(dim=1).values
     emax = (diag + radius).max(dim=1).values
     eye = torch.eye(n, dtype=fo.dtype, device=fo.device)
-    key = (nb, n, int(nocc), float(tol), str(fo.device), int(steps))
+    key = (nb, n, int(nocc), float(tol), str(fo.device), int(steps), gemm)
     if graphs is None:
         graphs = {}
     g = graphs.get(key)
@@ -294,13 +326,15 @@ def purify_sp2(fo: torch.Tensor, nocc: int, max_steps: int = 96, tol: float = 1e
         held = sum(3 * v.x.numel() * 8 for v in graphs.values())
         if held + 3 * nb * n * n * 8 > SP2_GRAPH_CACHE_BYTES:
             graphs.clear()
-        g = graphs[key] = _SP2Graph(nb, n, nocc, tol, fo.device, steps)
+        g = graphs[key] = _SP2Graph(nb, n, nocc, tol, fo.device, steps, gemm)
     torch.div(emax[:, None, None] * eye - fo, (emax - emin)[:, None, None], out=g.x)
     g.done.zero_()
     for _ in range(0, max_steps, int(steps)):
         g.run()
         if bool(g.done.all()):
             break
+    if gemm == "int8" and int(g.err.item()) != 0:
+        raise _lib.VqcError(6, f"tensor-core purification wait expired (code {int(g.err.item())})")
     return 0.5 * (g.x + g.x.transpose(1, 2))
 
 
@@ -670,11 +704,14 @@ def run_scf(chunk: Chunk, ints: ChunkIntegrals, xyz: torch.Tensor, *, precision:
     guess = torch.randn(nb, n, nocc, dtype=torch.float64, device=dev, generator=gen)
 
     sp2_graphs = _SP2_GRAPHS
+    # the FP64 comparator path keeps plain DGEMMs; the mixed path may take
+    # the sliced tensor-core products (FP64-accurate as well)
+    sp2_gemm = sched.sp2_gemm if precision == "mixed" else "fp64"
 
     def density_from(f, guess, tol=1e-11, noise_scale=0.3):
         with TIMER.stage("purify"):
             proj = purify_sp2(xo.transpose(1, 2) @ f @ xo, nocc, tol=tol, graphs=sp2_graphs,
-                              steps=sched.sp2_steps)
+                              steps=sched.sp2_steps, gemm=sp2_gemm)
         with TIMER.stage("occupied_factor"):
             co = occupied_factor(proj, guess, gen, noise_scale)  # orthonormal, orthogonal basis
         return 2.0 * (xo @ proj @ xo.transpose(1, 2)), co

@@ -13,7 +13,10 @@ the device that will run them and stored in a table
 * ``gram_waves``: the exchange Gram product splits its K range until about
   this many CTAs per SM exist (library knob ``VQC_TUNE_GRAM_WAVES``);
 * ``sp2_steps``: purification steps per captured CUDA graph (more steps mean
-  fewer host round trips, but converged molecules idle longer).
+  fewer host round trips, but converged molecules idle longer);
+* ``sp2_gemm``: how the mixed path forms the purification product X^2 --
+  batched FP64 GEMMs (``"fp64"``) or FP64-accurate sliced products on the
+  int8 tensor cores (``"int8"``).
 
     python -m vibeqc_b200.tuning [--count 256] [--out path]
 
@@ -34,6 +37,7 @@ TABLE_PATH = Path(__file__).resolve().parent / "data" / "tuning.json"
 WHITEN_CHOICES = ("int8", "fp64")
 GRAM_WAVES = (1, 2, 4, 8)
 SP2_STEPS = (4, 8, 16)
+SP2_GEMMS = ("fp64", "int8")
 
 
 @dataclass(frozen=True)
@@ -41,6 +45,7 @@ class Schedule:
     whiten: str = "int8"
     gram_waves: int = 2
     sp2_steps: int = 8
+    sp2_gemm: str = "fp64"
 
     def __post_init__(self):
         if self.whiten not in WHITEN_CHOICES:
@@ -49,6 +54,8 @@ class Schedule:
             raise ValueError("gram_waves must be in 1..64")
         if int(self.sp2_steps) < 2 or int(self.sp2_steps) % 2:
             raise ValueError("sp2_steps must be an even number >= 2")
+        if self.sp2_gemm not in SP2_GEMMS:
+            raise ValueError(f"sp2_gemm must be one of {SP2_GEMMS}")
 
 
 DEFAULT = Schedule()
@@ -189,7 +196,13 @@ def tune_chunk(chunk, xyz) -> tuple[Schedule, dict]:
         timings["sp2_steps"][str(n_steps)] = round(
             _time(lambda: purify_sp2(fo, chunk.nocc, graphs=graphs, steps=n_steps)), 3)
     steps_best = int(min(timings["sp2_steps"], key=timings["sp2_steps"].get))
-    return Schedule(whiten_best, waves_best, steps_best), timings
+    timings["sp2_gemm"] = {}
+    for gemm in SP2_GEMMS:
+        graphs = {}
+        timings["sp2_gemm"][gemm] = round(
+            _time(lambda: purify_sp2(fo, chunk.nocc, graphs=graphs, steps=steps_best, gemm=gemm)), 3)
+    gemm_best = min(timings["sp2_gemm"], key=timings["sp2_gemm"].get)
+    return Schedule(whiten_best, waves_best, steps_best, gemm_best), timings
 
 
 def autotune(systems, basis: str, auxiliary_basis: str, precision: str = "mixed") -> TuningTable:

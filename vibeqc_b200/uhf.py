@@ -229,7 +229,8 @@ def run_scf_uhf(chunk, ints, xyz: torch.Tensor, *, precision: str = "fp64",
             return torch.zeros_like(f), torch.zeros(nb, n, 0, dtype=f.dtype, device=dev)
         with TIMER.stage("purify"):
             proj = scfm.purify_sp2(xo.transpose(1, 2) @ f @ xo, nocc, tol=tol,
-                                   graphs=scfm._SP2_GRAPHS, steps=sched.sp2_steps)
+                                   graphs=scfm._SP2_GRAPHS, steps=sched.sp2_steps,
+                                   gemm=sched.sp2_gemm if precision == "mixed" else "fp64")
         with TIMER.stage("occupied_factor"):
             co = scfm.occupied_factor(proj, guess, gen, noise_scale)
         return xo @ proj @ xo.transpose(1, 2), co
