@@ -225,7 +225,13 @@ int vqc_sp2_update(const double* x, const double* x2, double* xout, int32_t nmol
  *     TF32-representable), and rho[mol][Q] += 2 sum_{mu,i} U C[mu][i];
  *     ct_hi/ct_lo = split C^T [mol][nocc][ld_ao] FP32, c_occ = C
  *     [mol][nao][nocc] FP64; o_pad = MMA N (round_up(nocc,16) <= 128).
- *     Reference src/scf/cuda/df_occupied_exchange.cpp:251-257 (U = B C).
+ *     With dens (D [mol][nao][nao] FP64, NULL to skip) the same pass also
+ *     adds the fitted density rho_dens[mol][Q] += sum_{mu,nu} B[mu][Q][nu]
+ *     D[mu][nu] (FP64 products of the exact FP32 B values; dens and rho_dens
+ *     both set or both NULL), so a build needs no separate fitted-density
+ *     pass over B.
+ *     Reference src/scf/cuda/df_occupied_exchange.cpp:251-257 (U = B C) and
+ *     src/scf/cuda/df_coulomb.cpp:38-57 (rho = B^T vec(D)).
  *   vqc_tc_gram: kout[mol] += U U^T over kdim = nocc * ld_aux from the split
  *     U (3xTF32, FP64 output); reference df_occupied_exchange.cpp:262-279.
  *   vqc_tc_gram_sym2: kout[mol] += A B^T + B A^T for two split operands of
@@ -259,7 +265,8 @@ int vqc_wait_selftest(int32_t budget_us, int32_t* error, void* stream);
 int vqc_tc_half_transform(const float* b_aux_major, int32_t nmol, int32_t nao, int32_t ld_ao,
                           int32_t naux, const float* ct_hi, const float* ct_lo,
                           const double* c_occ, int32_t nocc, int32_t o_pad, int32_t ld_aux,
-                          float* u_hi, float* u_lo, double* rho, int32_t* error, void* stream);
+                          float* u_hi, float* u_lo, double* rho, const double* dens,
+                          double* rho_dens, int32_t* error, void* stream);
 int vqc_tc_gram(const float* u_hi, const float* u_lo, int32_t nmol, int32_t nao, int32_t kdim,
                 double* kout, int32_t* error, void* stream);
 int vqc_tc_gram_sym2(const float* a_hi, const float* a_lo, const float* b_hi, const float* b_lo,

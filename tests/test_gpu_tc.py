@@ -36,9 +36,12 @@ def test_half_transform_and_gram(nb, n, x, o):
     u_lo = torch.zeros_like(u_hi)
     rho = torch.zeros(nb, x, dtype=torch.float64, device="cuda")
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    dm = torch.randn(nb, n, n, generator=g, device="cuda", dtype=torch.float64)
+    dm = 0.5 * (dm + dm.transpose(1, 2))
+    rho_d = torch.zeros(nb, x, dtype=torch.float64, device="cuda")
     _lib.call("vqc_tc_half_transform", b.data_ptr(), nb, n, ld, x, ct_hi.data_ptr(),
               ct_lo.data_ptr(), c.contiguous().data_ptr(), o, o_pad, ldq, u_hi.data_ptr(),
-              u_lo.data_ptr(), rho.data_ptr(), err.data_ptr(), st)
+              u_lo.data_ptr(), rho.data_ptr(), dm.data_ptr(), rho_d.data_ptr(), err.data_ptr(), st)
     torch.cuda.synchronize()
     assert int(err.item()) == 0
     assert torch.isfinite(u_hi).all() and torch.isfinite(u_lo).all()
@@ -55,6 +58,9 @@ def test_half_transform_and_gram(nb, n, x, o):
     assert (u[..., x:] == 0).all()
     ref_rho = 2.0 * torch.einsum("bmi,bmqi->bq", c, ref)
     assert (rho - ref_rho).abs().max().item() <= 5e-6 * ref_rho.abs().max().item()
+    # fitted density formed by the splitters from the exact FP32 B (FP64 sums)
+    ref_rd = torch.einsum("bmqn,bmn->bq", b64, dm)
+    assert (rho_d - ref_rd).abs().max().item() <= 1e-12 * ref_rd.abs().max().item()
 
     kdim = o * ldq
     k = torch.zeros(nb, n, n, dtype=torch.float64, device="cuda")
@@ -203,8 +209,13 @@ def test_unpack_aux_major_roundtrip():
 def test_bad_arguments_rejected():
     st = torch.cuda.current_stream().cuda_stream
     with pytest.raises(_lib.VqcError):
-        _lib.call("vqc_tc_half_transform", 0, 1, 8, 8, 8, 0, 0, 0, 4, 16, 8, 0, 0, 0, 0, st)
+        _lib.call("vqc_tc_half_transform", 0, 1, 8, 8, 8, 0, 0, 0, 4, 16, 8, 0, 0, 0, 0, 0, 0, st)
     x = torch.zeros(64, dtype=torch.float32, device="cuda")
     with pytest.raises(_lib.VqcError):  # o_pad above the supported tile
         _lib.call("vqc_tc_half_transform", x.data_ptr(), 1, 8, 8, 8, x.data_ptr(), x.data_ptr(),
-                  x.data_ptr(), 140, 144, 8, x.data_ptr(), x.data_ptr(), x.data_ptr(), x.data_ptr(), st)
+                  x.data_ptr(), 140, 144, 8, x.data_ptr(), x.data_ptr(), x.data_ptr(), 0, 0,
+                  x.data_ptr(), st)
+    with pytest.raises(_lib.VqcError):  # density without its output
+        _lib.call("vqc_tc_half_transform", x.data_ptr(), 1, 8, 8, 8, x.data_ptr(), x.data_ptr(),
+                  x.data_ptr(), 4, 16, 8, x.data_ptr(), x.data_ptr(), x.data_ptr(), x.data_ptr(), 0,
+                  x.data_ptr(), st)

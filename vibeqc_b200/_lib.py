@@ -124,7 +124,7 @@ _SIGNATURES = {
     "vqc_wait_selftest": ([ctypes.c_int32, _P, _P], ctypes.c_int),
     "vqc_tc_half_transform": ([_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                ctypes.c_int32, _P, _P, _P, ctypes.c_int32, ctypes.c_int32,
-                               ctypes.c_int32, _P, _P, _P, _P, _P], ctypes.c_int),
+                               ctypes.c_int32, _P, _P, _P, _P, _P, _P, _P], ctypes.c_int),
     "vqc_tc_gram": ([_P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _P, _P, _P],
                     ctypes.c_int),
     "vqc_tc_gram_sym2": ([_P, _P, _P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _P,

@@ -156,6 +156,8 @@ struct HalfParams {
   float* u_lo;
   double* rho;
   const double* cvec;
+  const double* dens;  // optional D[mol][mu][nu]: the splitters also form rho_dens
+  double* rho_dens;    // rho_dens[mol][Q] += sum_{mu,nu} B[mu][Q][nu] D[mu][nu] (FP64)
   int* error;
 };
 
@@ -228,7 +230,39 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
     const int ts = tid - 32;
     int g = 0;
     const int i0 = blockIdx.x * p.per_cta, i1 = min(p.nitems, i0 + p.per_cta);
+    // With p.dens the splitters also form the fitted density from the exact
+    // FP32 values they split: rho_dens[Q] += sum_nu B[mu][Q][nu] D[mu][nu] in
+    // FP64.  Float4 k of a 128-byte-swizzled stage holds row r = k / 8 and
+    // logical chunk (k % 8) ^ (r % 8); this thread's rows are ts / 8 + 32 i
+    // (i < 4), all in the same chunk, so its four nu are fixed per K-block and
+    // the eight lanes sharing a row cover its 32 columns.
+    static_assert((C::A_BYTES / 16) % (32 * kSplitWarps) == 0 && kSplitWarps % 2 == 0,
+                  "each splitter thread owns whole float4 rows in one swizzle chunk");
+    constexpr int kRowsPerThread = C::A_BYTES / 16 / (32 * kSplitWarps);
+    const int chunk = (ts & 7) ^ ((ts >> 3) & 7);
+    double racc[kRowsPerThread];
+#pragma unroll
+    for (int i = 0; i < kRowsPerThread; ++i) racc[i] = 0.0;
+    int rkey = -1;
     for (int item = i0; item < i1; ++item) {
+      const int mu = item % p.nao, key = item / p.nao;  // key = mol * nqt + qt
+      if (p.dens && key != rkey) {
+        if (rkey >= 0) {
+#pragma unroll
+          for (int i = 0; i < kRowsPerThread; ++i) {
+            double v = racc[i];
+            v += __shfl_xor_sync(0xffffffffu, v, 1);
+            v += __shfl_xor_sync(0xffffffffu, v, 2);
+            v += __shfl_xor_sync(0xffffffffu, v, 4);
+            const int qrow = (rkey % p.nqt) * BM + (ts >> 3) + 32 * kSplitWarps / 8 * i;
+            if ((ts & 7) == 0 && qrow < p.naux)
+              atomicAdd(p.rho_dens + (size_t)(rkey / p.nqt) * p.naux + qrow, v);
+            racc[i] = 0.0;
+          }
+        }
+        rkey = key;
+      }
+      const double* drow = p.dens ? p.dens + ((size_t)(key / p.nqt) * p.nao + mu) * p.nao : nullptr;
       for (int kb = 0; kb < nk; ++kb, ++g) {
         const int s = g % S;
         // every lane waits; the warp leaves together (no lane may skip a
@@ -240,9 +274,21 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
         if (ts == 0) *reinterpret_cast<volatile int*>(&ctrl->consumed) = g + 1;
         float4* a = reinterpret_cast<float4*>(stage(s));
         float4* alo = reinterpret_cast<float4*>(stage(s) + C::A_BYTES);
-#pragma unroll 4
-        for (int k = ts; k < C::A_BYTES / 16; k += 32 * kSplitWarps) {
+        double w0 = 0.0, w1 = 0.0, w2 = 0.0, w3 = 0.0;
+        if (drow) {
+          const int nu = kb * BK + 4 * chunk;
+          if (nu < p.nao) w0 = __ldg(drow + nu);
+          if (nu + 1 < p.nao) w1 = __ldg(drow + nu + 1);
+          if (nu + 2 < p.nao) w2 = __ldg(drow + nu + 2);
+          if (nu + 3 < p.nao) w3 = __ldg(drow + nu + 3);
+        }
+#pragma unroll
+        for (int i = 0; i < kRowsPerThread; ++i) {
+          const int k = ts + i * 32 * kSplitWarps;
           float4 v = a[k], lo;
+          if (drow)
+            racc[i] = fma((double)v.x, w0, fma((double)v.y, w1,
+                      fma((double)v.z, w2, fma((double)v.w, w3, racc[i]))));
           split4(v, lo);
           a[k] = v;
           alo[k] = lo;
@@ -250,6 +296,18 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncwarp();
         if (lane == 0) mbar_arrive(conv0 + 8 * s);
+      }
+    }
+    if (p.dens && rkey >= 0) {
+#pragma unroll
+      for (int i = 0; i < kRowsPerThread; ++i) {
+        double v = racc[i];
+        v += __shfl_xor_sync(0xffffffffu, v, 1);
+        v += __shfl_xor_sync(0xffffffffu, v, 2);
+        v += __shfl_xor_sync(0xffffffffu, v, 4);
+        const int qrow = (rkey % p.nqt) * BM + (ts >> 3) + 32 * kSplitWarps / 8 * i;
+        if ((ts & 7) == 0 && qrow < p.naux)
+          atomicAdd(p.rho_dens + (size_t)(rkey / p.nqt) * p.naux + qrow, v);
       }
     }
   split_done:;
@@ -675,10 +733,11 @@ extern "C" int vqc_tc_half_transform(const float* b_aux_major, int32_t nmol, int
                                      int32_t ld_ao, int32_t naux, const float* ct_hi,
                                      const float* ct_lo, const double* c_occ, int32_t nocc,
                                      int32_t o_pad, int32_t ld_aux, float* u_hi, float* u_lo,
-                                     double* rho, int32_t* error, void* stream) {
+                                     double* rho, const double* dens, double* rho_dens,
+                                     int32_t* error, void* stream) {
   if (!b_aux_major || !ct_hi || !ct_lo || !c_occ || !u_hi || !u_lo || nmol <= 0 || nao <= 0 ||
       naux <= 0 || nocc <= 0 || o_pad < nocc || o_pad % 16 || o_pad > 128 || ld_ao < nao ||
-      ld_aux < naux || ld_aux % 4)
+      ld_aux < naux || ld_aux % 4 || (dens != nullptr) != (rho_dens != nullptr))
     return fail(VQC_STATUS_INVALID_ARGUMENT, "half_transform: bad argument");
   CUtensorMap ta, th, tl;
   int st = make_map(&ta, b_aux_major, nao, ld_ao, naux, nmol * nao, BM);
@@ -701,6 +760,8 @@ extern "C" int vqc_tc_half_transform(const float* b_aux_major, int32_t nmol, int
   p.u_lo = u_lo;
   p.rho = rho;
   p.cvec = c_occ;
+  p.dens = dens;
+  p.rho_dens = rho_dens;
   p.error = error;
   cudaStream_t s = (cudaStream_t)stream;
   switch (o_pad) {

@@ -125,7 +125,6 @@ class MixedBuilder:
         self.u_hi = torch.zeros(nb, n, nocc, self.ldq, dtype=torch.float32, device=dev)
         self.u_lo = torch.zeros_like(self.u_hi)
         self.rho = torch.empty(nb, x, dtype=torch.float64, device=dev)
-        self.rho_part = torch.empty(nb, n, x, dtype=torch.float64, device=dev)
         # the FP64 whitened tensor stays resident (full rows: the anchor's half
         # transform is then one plain GEMM per molecule, measured 2.6x faster
         # than gathering from the packed rows)
@@ -140,8 +139,10 @@ class MixedBuilder:
             raise self._lib.VqcError(6, f"tensor-core kernel wait expired (code {int(self.err.item())})")
 
     def _half(self, c_occ: torch.Tensor, cvec: torch.Tensor | None = None,
-              rho: torch.Tensor | None = None):
-        """U = B c_occ into u_hi/u_lo; rho += 2 sum_{mu,i} U cvec (when given)."""
+              rho: torch.Tensor | None = None, dens: torch.Tensor | None = None,
+              rho_dens: torch.Tensor | None = None):
+        """U = B c_occ into u_hi/u_lo; rho += 2 sum_{mu,i} U cvec (when given);
+        rho_dens += B^T vec(dens) from the same pass over B (when given)."""
         nb, n, o = self.nb, self.n, self.nocc
         ct = torch.zeros(nb, o, self.ld, dtype=torch.float32, device=c_occ.device)
         ct[:, :, :n] = c_occ.transpose(1, 2)
@@ -157,23 +158,27 @@ class MixedBuilder:
             self._lib.call("vqc_tc_half_transform", self.b.data_ptr(), nb, n, self.ld, self.x,
                            ct_hi.data_ptr(), ct_lo.data_ptr(), c64.data_ptr(), o, self.o_pad,
                            self.ldq, self.u_hi.data_ptr(), self.u_lo.data_ptr(),
-                           0 if rho is None else rho.data_ptr(), self.err.data_ptr(), self.st)
+                           0 if rho is None else rho.data_ptr(),
+                           0 if dens is None else dens.data_ptr(),
+                           0 if rho_dens is None else rho_dens.data_ptr(),
+                           self.err.data_ptr(), self.st)
 
     def build(self, d: torch.Tensor, c_occ: torch.Tensor, with_j: bool = True):
         nb, n = self.nb, self.n
-        self._half(c_occ)
         j = None
         if with_j:
+            # the fitted density rho = B^T vec(D) comes from the half
+            # transform's own pass over the FP32 B (FP64 products of the exact
+            # FP32 values, no tensor-core accumulation error in J), then J = B rho
+            dd = d.contiguous()
+            self.rho.zero_()
+            self._half(c_occ, dens=dd, rho_dens=self.rho)
             j = torch.empty(nb, n, n, dtype=torch.float64, device=d.device)
             with TIMER.stage("J_fp32"):
-                # fitted density from the FP32 B with FP64 accumulation (no
-                # tensor-core accumulation error in J), then J = B rho
-                dd = d.contiguous()
-                self._lib.call("vqc_fitted_density_fp32", self.b.data_ptr(), dd.data_ptr(), nb, n,
-                               self.ld, self.x, self.rho_part.data_ptr(), self.rho.data_ptr(),
-                               self.st)
                 self._lib.call("vqc_coulomb_fp32", self.b.data_ptr(), self.rho.data_ptr(), nb, n,
                                self.ld, self.x, j.data_ptr(), self.st)
+        else:
+            self._half(c_occ)
         k = torch.zeros(nb, n, n, dtype=torch.float64, device=d.device)
         COUNTERS["k_flops"] += nb * self.x * self.nocc * n * (n + 1)
         with TIMER.stage("K_gram_tc"):
@@ -197,7 +202,6 @@ class MixedBuilder:
         """Free the FP32 tensor and the split U/V buffers once the SCF is done."""
         self.b = self.u_hi = self.u_lo = None
         self.v_hi = self.v_lo = None
-        self.rho_part = None
 
     # -- incremental builds about an FP64 anchor ---------------------------
     #
