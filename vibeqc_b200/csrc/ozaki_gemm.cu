@@ -152,6 +152,10 @@ __global__ void __launch_bounds__(kThreads, 1)
   const uint32_t af0 = smem_u32(ctrl->a_full), ae0 = smem_u32(ctrl->a_empty);
   const uint32_t bf0 = smem_u32(ctrl->b_full), be0 = smem_u32(ctrl->b_empty);
   const uint32_t accf = smem_u32(&ctrl->acc_full), drain = smem_u32(&ctrl->drain);
+  // the tile's column exponents, read by every epilogue thread (shared-memory
+  // broadcast instead of one global load per column and thread)
+  __shared__ int s_eb[BN];
+  if (tid < BN) s_eb[tid] = n0 + tid < p.n ? p.b_exp[(long long)z * p.n + n0 + tid] : 0;
   if (tid == 0) {
     for (int s = 0; s < kARing; ++s) {
       mbar_init(af0 + 8 * s, 1);
@@ -277,14 +281,21 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (int c = 0; c < BN; ++c) acc[c] = fma((double)v[c], scale, acc[c]);
       }
       // scale by 2^(ea + eb) in one step (no intermediate underflow), stage the
-      // warp's 32 rows in the idle A ring, then store whole rows
+      // warp's 32 rows in the idle A ring, then store whole rows.  For a normal
+      // power of two the product with 2^e (built from its exponent bits) is
+      // exactly ldexp (one rounding, only when the result is subnormal);
+      // exponents outside the normal range take ldexp itself.
       const int ea = row < p.m ? p.a_exp[(long long)z * p.m + row] : 0;
-      const int* eb = p.b_exp + (long long)z * p.n;
       double* stage = reinterpret_cast<double*>(abuf) + (size_t)(warp - 2) * 32 * kStageLd;
 #pragma unroll
       for (int c = 0; c < BN; ++c) {
-        const int col = n0 + c;
-        stage[lane * kStageLd + c] = col < p.n ? ldexp(acc[c], ea + eb[col]) : 0.0;
+        const int e = ea + s_eb[c];
+        double v = acc[c];
+        if (e >= -1022 && e <= 1023)
+          v *= __longlong_as_double((long long)(e + 1023) << 52);
+        else
+          v = ldexp(v, e);
+        stage[lane * kStageLd + c] = n0 + c < p.n ? v : 0.0;
       }
       __syncwarp();
       const int rbase = m0 + q * 32;

@@ -244,6 +244,19 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
 #pragma unroll
     for (int i = 0; i < kRowsPerThread; ++i) racc[i] = 0.0;
     int rkey = -1;
+    // density weights D[mol][mu][nu] of (item, K-block): this thread's four nu
+    auto load_weights = [&](int it, int kb, double (&w)[4]) {
+      w[0] = w[1] = w[2] = w[3] = 0.0;
+      if (!p.dens || it >= i1) return;
+      const int m = it % p.nao, key = it / p.nao;
+      const double* drow = p.dens + ((size_t)(key / p.nqt) * p.nao + m) * p.nao;
+      const int nu = kb * BK + 4 * chunk;
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (nu + e < p.nao) w[e] = __ldg(drow + nu + e);
+    };
+    double wn[4];
+    load_weights(i0, 0, wn);
     for (int item = i0; item < i1; ++item) {
       const int mu = item % p.nao, key = item / p.nao;  // key = mol * nqt + qt
       if (p.dens && key != rkey) {
@@ -262,9 +275,14 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
         }
         rkey = key;
       }
-      const double* drow = p.dens ? p.dens + ((size_t)(key / p.nqt) * p.nao + mu) * p.nao : nullptr;
+      (void)mu;
       for (int kb = 0; kb < nk; ++kb, ++g) {
         const int s = g % S;
+        // this K-block's density weights were loaded one step ahead; fetch
+        // the next step's now, before the barrier wait hides their latency
+        const double w0 = wn[0], w1 = wn[1], w2 = wn[2], w3 = wn[3];
+        if (kb + 1 < nk) load_weights(item, kb + 1, wn);
+        else load_weights(item + 1, 0, wn);
         // every lane waits; the warp leaves together (no lane may skip a
         // later warp-collective alone)
         if (!__all_sync(0xffffffffu, mbar_wait(full0 + 8 * s, (g / S) & 1, ab))) {
@@ -274,19 +292,11 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
         if (ts == 0) *reinterpret_cast<volatile int*>(&ctrl->consumed) = g + 1;
         float4* a = reinterpret_cast<float4*>(stage(s));
         float4* alo = reinterpret_cast<float4*>(stage(s) + C::A_BYTES);
-        double w0 = 0.0, w1 = 0.0, w2 = 0.0, w3 = 0.0;
-        if (drow) {
-          const int nu = kb * BK + 4 * chunk;
-          if (nu < p.nao) w0 = __ldg(drow + nu);
-          if (nu + 1 < p.nao) w1 = __ldg(drow + nu + 1);
-          if (nu + 2 < p.nao) w2 = __ldg(drow + nu + 2);
-          if (nu + 3 < p.nao) w3 = __ldg(drow + nu + 3);
-        }
 #pragma unroll
         for (int i = 0; i < kRowsPerThread; ++i) {
           const int k = ts + i * 32 * kSplitWarps;
           float4 v = a[k], lo;
-          if (drow)
+          if (p.dens)
             racc[i] = fma((double)v.x, w0, fma((double)v.y, w1,
                       fma((double)v.z, w2, fma((double)v.w, w3, racc[i]))));
           split4(v, lo);
