@@ -227,6 +227,158 @@ __global__ void __launch_bounds__(round32(Int3cCfg<LA, LB, LC, SPH>::THREADS),
 }
 
 // ---------------------------------------------------------------------------
+// 3-centre derivative contraction, root-parallel form for classes with few
+// Cartesian products: one thread per (shell pair, aux shell, Rys root) holds
+// the weights of every aux component, evaluates its own root and one
+// vertical table per direction, and contracts all components from it (the
+// per-component kernel above repeats the roots and vertical tables for each
+// component).  The roots of a slot are adjacent lanes with the same atoms,
+// so the warp-segmented atomics sum them.  Same CTA work decomposition as the
+// value kernels (the plan's launch tables are shared).
+// ---------------------------------------------------------------------------
+
+__host__ __device__ constexpr int nroots_g3c(int la, int lb, int lc) { return (la + lb + lc + 1) / 2 + 1; }
+__host__ __device__ constexpr bool use_root_parallel_g3c(int la, int lb, int lc) {
+  return lc >= 1 && ncart(la) * ncart(lb) * ncart(lc) <= 36;
+}
+__host__ __device__ constexpr int rp_threads_g3c(int la, int lb, int lc, bool sph) {
+  return round32(slots3c(la, lb, lc, sph) * nroots_g3c(la, lb, lc));
+}
+
+template <int LA, int LB, int LC, bool SPH>
+__global__ void __launch_bounds__(rp_threads_g3c(LA, LB, LC, SPH))
+    grad3c_rp_kernel(DevBasis orb, DevBasis aux, const double* __restrict__ xyz,
+                     const DevMol* __restrict__ mols, const int2* __restrict__ pairs,
+                     const ClassMol* __restrict__ cms, int ncm, const double* __restrict__ abar,
+                     double* __restrict__ grad) {
+  using C = Int3cCfg<LA, LB, LC, SPH>;
+  constexpr int NCA = ncart(LA), NCB = ncart(LB), NCC = ncart(LC);
+  constexpr int NOA = C::NOA, NOB = C::NOB, NOC = C::NOC;
+  constexpr int NR = nroots_g3c(LA, LB, LC);
+  constexpr int LAB1 = LA + LB + 2;  // vertical table height for the raised a and b
+  constexpr int MODE = SPH ? 0 : 1;
+  constexpr Cart<LA> ca{};
+  constexpr Cart<LB> cb{};
+  constexpr Cart<LC> cc{};
+
+  const ClassMol cm = cms[find_cm_g(cms, ncm, blockIdx.x)];
+  const int t0 = (blockIdx.x - cm.chunk_begin) * C::SLOTS;
+  const int slot = threadIdx.x / NR, r = threadIdx.x % NR;
+  const int t = t0 + slot;
+  const bool valid = slot < C::SLOTS && t < cm.ntriples;
+  double gA[3] = {0.0, 0.0, 0.0}, gB[3] = {0.0, 0.0, 0.0};
+  int atomA = -1, atomB = -1, atomC = -1;
+  if (valid) {
+    const int2 pr = pairs[cm.pair_begin + t / cm.naux];
+    const int sc = cm.aux_begin + t % cm.naux;
+    atomA = orb.atom[pr.x];
+    atomB = orb.atom[pr.y];
+    atomC = aux.atom[sc];
+    if (!(atomA == atomB && atomB == atomC)) {
+      const DevMol mol = mols[cm.mol];
+      // weights of every Cartesian aux component, Cartesian in a and b
+      double wc[NCC][NCA][NCB];
+      const int fa = orb.func_off[pr.x], fb = orb.func_off[pr.y], fc = aux.func_off[sc];
+      {
+        double wk[NOA][NOB][NOC];
+#pragma unroll
+        for (int i = 0; i < NOA; ++i)
+#pragma unroll
+          for (int j = 0; j < NOB; ++j) {
+            const long long mu = fa + i, nu = fb + j;
+            const long long hi = mu > nu ? mu : nu, lo = mu > nu ? nu : mu;
+            const double* row = abar + mol.a_off + (hi * (hi + 1) / 2 + lo) * mol.naux + fc;
+#pragma unroll
+            for (int k = 0; k < NOC; ++k) wk[i][j][k] = __ldg(row + k);
+          }
+#pragma unroll
+        for (int z = 0; z < NCC; ++z) {
+          double wsph[NOA][NOB];
+#pragma unroll
+          for (int i = 0; i < NOA; ++i)
+#pragma unroll
+            for (int j = 0; j < NOB; ++j) {
+              double s = 0.0;
+#pragma unroll
+              for (int k = 0; k < NOC; ++k) s = fma(c_trans[MODE][LC][k][z], wk[i][j][k], s);
+              wsph[i][j] = s;
+            }
+          weights_to_cart<LA, LB, NOA, NOB>(MODE, wsph, wc[z]);
+        }
+      }
+      const double pair_factor = (pr.x == pr.y) ? 1.0 : 2.0;
+      const double* A = xyz + 3 * atomA;
+      const double* B = xyz + 3 * atomB;
+      const double* Cc = xyz + 3 * atomC;
+      const double ab[3] = {A[0] - B[0], A[1] - B[1], A[2] - B[2]};
+      const double rab2 = ab[0] * ab[0] + ab[1] * ab[1] + ab[2] * ab[2];
+      const int pa0 = orb.prim_off[pr.x], na = orb.nprim[pr.x];
+      const int pb0 = orb.prim_off[pr.y], nb = orb.nprim[pr.y];
+      const int pc0 = aux.prim_off[sc], nc = aux.nprim[sc];
+      for (int ia = 0; ia < na; ++ia) {
+        const double a = orb.exps[pa0 + ia], ca_ = orb.coefs[pa0 + ia];
+        for (int ib = 0; ib < nb; ++ib) {
+          const double b = orb.exps[pb0 + ib], cb_ = orb.coefs[pb0 + ib];
+          const double p = a + b, ip = 1.0 / p;
+          const double kab = exp(-a * b * ip * rab2) * ca_ * cb_;
+          const double P[3] = {(a * A[0] + b * B[0]) * ip, (a * A[1] + b * B[1]) * ip,
+                               (a * A[2] + b * B[2]) * ip};
+          for (int ic = 0; ic < nc; ++ic) {
+            const double g = aux.exps[pc0 + ic], cg = aux.coefs[pc0 + ic];
+            const double pq = p + g, ipq = 1.0 / pq;
+            const double PQ[3] = {P[0] - Cc[0], P[1] - Cc[1], P[2] - Cc[2]};
+            const double tt = p * g * ipq * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
+            const double pref =
+                2.0 * kPi * kPi * sqrt(kPi) * ip / g * sqrt(ipq) * kab * cg * pair_factor;
+            double ur, wr0;
+            rys_root_one<NR>(tt, r, ur, wr0);
+            const double qf = g * ipq * ur, pf = p * ipq * ur;
+            const double b00 = 0.5 * ipq * ur, b10 = 0.5 * ip * (1.0 - qf),
+                         b01 = 0.5 / g * (1.0 - pf);
+            double gx[LAB1 + 1][LC + 1], gy[LAB1 + 1][LC + 1], gz[LAB1 + 1][LC + 1];
+            rys_vrr<LAB1, LC>(P[0] - A[0] - qf * PQ[0], pf * PQ[0], b10, b01, b00, gx);
+            rys_vrr<LAB1, LC>(P[1] - A[1] - qf * PQ[1], pf * PQ[1], b10, b01, b00, gy);
+            rys_vrr<LAB1, LC>(P[2] - A[2] - qf * PQ[2], pf * PQ[2], b10, b01, b00, gz);
+            const double wr = pref * wr0;
+#pragma unroll
+            for (int z = 0; z < NCC; ++z) {
+              double ix[LA + 2][LB + 2], iy[LA + 2][LB + 2], iz[LA + 2][LB + 2];
+              rys_hrr_col<LA + 1, LB + 1, LC>(gx, cc.x[z], ab[0], ix);
+              rys_hrr_col<LA + 1, LB + 1, LC>(gy, cc.y[z], ab[1], iy);
+              rys_hrr_col<LA + 1, LB + 1, LC>(gz, cc.z[z], ab[2], iz);
+#pragma unroll
+              for (int i = 0; i < NCA; ++i)
+#pragma unroll
+                for (int j = 0; j < NCB; ++j) {
+                  const int ax = ca.x[i], ay = ca.y[i], az = ca.z[i];
+                  const int bx = cb.x[j], by = cb.y[j], bz = cb.z[j];
+                  const double x0 = ix[ax][bx], y0 = iy[ay][by], z0 = iz[az][bz];
+                  const double dax = 2.0 * a * ix[ax + 1][bx] - (ax ? ax * ix[ax ? ax - 1 : 0][bx] : 0.0);
+                  const double day = 2.0 * a * iy[ay + 1][by] - (ay ? ay * iy[ay ? ay - 1 : 0][by] : 0.0);
+                  const double daz = 2.0 * a * iz[az + 1][bz] - (az ? az * iz[az ? az - 1 : 0][bz] : 0.0);
+                  const double dbx = 2.0 * b * ix[ax][bx + 1] - (bx ? bx * ix[ax][bx ? bx - 1 : 0] : 0.0);
+                  const double dby = 2.0 * b * iy[ay][by + 1] - (by ? by * iy[ay][by ? by - 1 : 0] : 0.0);
+                  const double dbz = 2.0 * b * iz[az][bz + 1] - (bz ? bz * iz[az][bz ? bz - 1 : 0] : 0.0);
+                  const double ww = wr * wc[z][i][j];
+                  gA[0] = fma(ww, dax * y0 * z0, gA[0]);
+                  gA[1] = fma(ww, x0 * day * z0, gA[1]);
+                  gA[2] = fma(ww, x0 * y0 * daz, gA[2]);
+                  gB[0] = fma(ww, dbx * y0 * z0, gB[0]);
+                  gB[1] = fma(ww, x0 * dby * z0, gB[1]);
+                  gB[2] = fma(ww, x0 * y0 * dbz, gB[2]);
+                }
+            }
+          }
+        }
+      }
+    }
+  }
+  warp_seg_add(grad, atomA, gA[0], gA[1], gA[2]);
+  warp_seg_add(grad, atomB, gB[0], gB[1], gB[2]);
+  warp_seg_add(grad, atomC, -(gA[0] + gB[0]), -(gA[1] + gB[1]), -(gA[2] + gB[2]));
+}
+
+// ---------------------------------------------------------------------------
 // 2-centre derivative contraction
 // ---------------------------------------------------------------------------
 
@@ -482,8 +634,13 @@ __global__ void __launch_bounds__(128)
 
 template <int LA, int LB, int LC, bool SPH>
 static void glaunch3(const ClassLaunch& cl, const KernelArgs& k, cudaStream_t st) {
-  grad3c_kernel<LA, LB, LC, SPH><<<cl.nblocks, round32(Int3cCfg<LA, LB, LC, SPH>::THREADS), 0, st>>>(
-      k.orb, k.aux, k.xyz, k.mols, cl.pairs, cl.cms, cl.ncm, k.w1, k.grad);
+  if constexpr (use_root_parallel_g3c(LA, LB, LC)) {
+    grad3c_rp_kernel<LA, LB, LC, SPH><<<cl.nblocks, rp_threads_g3c(LA, LB, LC, SPH), 0, st>>>(
+        k.orb, k.aux, k.xyz, k.mols, cl.pairs, cl.cms, cl.ncm, k.w1, k.grad);
+  } else {
+    grad3c_kernel<LA, LB, LC, SPH><<<cl.nblocks, round32(Int3cCfg<LA, LB, LC, SPH>::THREADS), 0, st>>>(
+        k.orb, k.aux, k.xyz, k.mols, cl.pairs, cl.cms, cl.ncm, k.w1, k.grad);
+  }
 }
 
 template <int LA, int LC, bool SPH>

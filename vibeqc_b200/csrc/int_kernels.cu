@@ -179,6 +179,153 @@ __global__ void __launch_bounds__(Int3cCfg<LA, LB, LC, SPH>::THREADS, min_ctas3c
 }
 
 // ---------------------------------------------------------------------------
+// 3-centre (mu nu | P), root-parallel form for classes with few Cartesian
+// products: one thread per (shell pair, aux shell, Rys root) instead of per
+// Cartesian aux component.  The per-component kernel above evaluates the
+// roots and the vertical tables once per component (NCC times the same
+// work); here each thread evaluates only its own root and one vertical table
+// per direction, then forms every aux component from it.  The roots' partial
+// sums meet in shared memory; the epilogue is the component kernel's.  Same
+// CTA work decomposition (SLOTS triples per CTA), so both forms share the
+// plan's launch tables.
+// ---------------------------------------------------------------------------
+
+__host__ __device__ constexpr int nroots3c(int la, int lb, int lc) { return (la + lb + lc) / 2 + 1; }
+// classes whose per-thread accumulators stay small and whose per-root
+// partials fit the static shared-memory limit
+__host__ __device__ constexpr bool use_root_parallel3c(int la, int lb, int lc, bool sph) {
+  return lc >= 1 && ncart(la) * ncart(lb) * ncart(lc) <= 36 &&
+         slots3c(la, lb, lc, sph) * nroots3c(la, lb, lc) * ncart(lc) * out_count(la, sph) *
+                 out_count(lb, sph) * 8 <= 40 * 1024;
+}
+__host__ __device__ constexpr int rp_threads3c(int la, int lb, int lc, bool sph) {
+  return (slots3c(la, lb, lc, sph) * nroots3c(la, lb, lc) + 31) / 32 * 32;
+}
+
+template <int LA, int LB, int LC, bool SPH>
+__global__ void __launch_bounds__(rp_threads3c(LA, LB, LC, SPH))
+    int3c_rp_kernel(DevBasis orb, DevBasis aux, const double* __restrict__ xyz,
+                    const DevMol* __restrict__ mols, const int2* __restrict__ pairs,
+                    const ClassMol* __restrict__ cms, int ncm, double* __restrict__ out) {
+  using C = Int3cCfg<LA, LB, LC, SPH>;
+  constexpr int NCA = ncart(LA), NCB = ncart(LB), NCC = ncart(LC);
+  constexpr int NOA = C::NOA, NOB = C::NOB, NOC = C::NOC;
+  constexpr int NR = nroots3c(LA, LB, LC);
+  constexpr int LAB = LA + LB;
+  constexpr int MODE = SPH ? 0 : 1;
+  constexpr Cart<LA> ca{};
+  constexpr Cart<LB> cb{};
+  constexpr Cart<LC> cc{};
+  __shared__ double part[C::SLOTS][NR][NCC][NOA * NOB];
+
+  const ClassMol cm = cms[find_cm(cms, ncm, blockIdx.x)];
+  const int t0 = (blockIdx.x - cm.chunk_begin) * C::SLOTS;
+  const int slot = threadIdx.x / NR, r = threadIdx.x % NR;
+  const int t = t0 + slot;
+  const bool valid = slot < C::SLOTS && t < cm.ntriples;
+
+  double acc[NCC][NCA][NCB];
+#pragma unroll
+  for (int k = 0; k < NCC; ++k)
+#pragma unroll
+    for (int i = 0; i < NCA; ++i)
+#pragma unroll
+      for (int j = 0; j < NCB; ++j) acc[k][i][j] = 0.0;
+
+  if (valid) {
+    const int2 pr = pairs[cm.pair_begin + t / cm.naux];
+    const int sc = cm.aux_begin + t % cm.naux;
+    const double* A = xyz + 3 * orb.atom[pr.x];
+    const double* B = xyz + 3 * orb.atom[pr.y];
+    const double* Cc = xyz + 3 * aux.atom[sc];
+    const double ab[3] = {A[0] - B[0], A[1] - B[1], A[2] - B[2]};
+    const double rab2 = ab[0] * ab[0] + ab[1] * ab[1] + ab[2] * ab[2];
+    const int pa0 = orb.prim_off[pr.x], na = orb.nprim[pr.x];
+    const int pb0 = orb.prim_off[pr.y], nb = orb.nprim[pr.y];
+    const int pc0 = aux.prim_off[sc], nc = aux.nprim[sc];
+    for (int ia = 0; ia < na; ++ia) {
+      const double a = orb.exps[pa0 + ia], ca_ = orb.coefs[pa0 + ia];
+      for (int ib = 0; ib < nb; ++ib) {
+        const double b = orb.exps[pb0 + ib], cb_ = orb.coefs[pb0 + ib];
+        const double p = a + b, ip = 1.0 / p;
+        const double kab = exp(-a * b * ip * rab2) * ca_ * cb_;
+        const double P[3] = {(a * A[0] + b * B[0]) * ip, (a * A[1] + b * B[1]) * ip,
+                             (a * A[2] + b * B[2]) * ip};
+        for (int ic = 0; ic < nc; ++ic) {
+          const double g = aux.exps[pc0 + ic], cg = aux.coefs[pc0 + ic];
+          const double pq = p + g, ipq = 1.0 / pq;
+          const double PQ[3] = {P[0] - Cc[0], P[1] - Cc[1], P[2] - Cc[2]};
+          const double tt = p * g * ipq * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
+          const double pref = 2.0 * kPi * kPi * sqrt(kPi) * ip / g * sqrt(ipq) * kab * cg;
+          double ur, wr0;
+          rys_root_one<NR>(tt, r, ur, wr0);
+          const double qf = g * ipq * ur, pf = p * ipq * ur;
+          const double b00 = 0.5 * ipq * ur;
+          const double b10 = 0.5 * ip * (1.0 - qf);
+          const double b01 = 0.5 / g * (1.0 - pf);
+          double gx[LAB + 1][LC + 1], gy[LAB + 1][LC + 1], gz[LAB + 1][LC + 1];
+          rys_vrr<LAB, LC>(P[0] - A[0] - qf * PQ[0], pf * PQ[0], b10, b01, b00, gx);
+          rys_vrr<LAB, LC>(P[1] - A[1] - qf * PQ[1], pf * PQ[1], b10, b01, b00, gy);
+          rys_vrr<LAB, LC>(P[2] - A[2] - qf * PQ[2], pf * PQ[2], b10, b01, b00, gz);
+          const double wr = pref * wr0;
+#pragma unroll
+          for (int k = 0; k < NCC; ++k) {
+            double ix[LA + 1][LB + 1], iy[LA + 1][LB + 1], iz[LA + 1][LB + 1];
+            rys_hrr_col<LA, LB, LC>(gx, cc.x[k], ab[0], ix);
+            rys_hrr_col<LA, LB, LC>(gy, cc.y[k], ab[1], iy);
+            rys_hrr_col<LA, LB, LC>(gz, cc.z[k], ab[2], iz);
+#pragma unroll
+            for (int i = 0; i < NCA; ++i)
+#pragma unroll
+              for (int j = 0; j < NCB; ++j)
+                acc[k][i][j] = fma(wr * ix[ca.x[i]][cb.x[j]], iy[ca.y[i]][cb.y[j]] * iz[ca.z[i]][cb.z[j]],
+                                   acc[k][i][j]);
+          }
+        }
+      }
+    }
+  }
+  if (slot < C::SLOTS) {
+#pragma unroll
+    for (int k = 0; k < NCC; ++k) {
+      double wsph[NOA][NOB];
+      transform_ab<LA, LB, NOA, NOB>(MODE, acc[k], wsph);
+#pragma unroll
+      for (int i = 0; i < NOA; ++i)
+#pragma unroll
+        for (int j = 0; j < NOB; ++j) part[slot][r][k][i * NOB + j] = wsph[i][j];
+    }
+  }
+  __syncthreads();
+
+  const DevMol mol = mols[cm.mol];
+  constexpr int PER_IJ = C::SLOTS * NOC;
+  constexpr int TOTAL = PER_IJ * NOA * NOB;
+  for (int o = threadIdx.x; o < TOTAL; o += blockDim.x) {
+    const int ij = o / PER_IJ, rr = o - ij * PER_IJ;
+    const int s = rr / NOC, k = rr - s * NOC;
+    const int ts = t0 + s;
+    if (ts >= cm.ntriples) continue;
+    const int2 pr = pairs[cm.pair_begin + ts / cm.naux];
+    const int sc = cm.aux_begin + ts % cm.naux;
+    const int i = ij / NOB, j = ij - i * NOB;
+    const int mu = orb.func_off[pr.x] + i, nu = orb.func_off[pr.y] + j;
+    if (pr.x == pr.y && mu < nu) continue;
+    double v = 0.0;
+#pragma unroll
+    for (int z = 0; z < NCC; ++z) {
+      double sz = 0.0;
+#pragma unroll
+      for (int q = 0; q < NR; ++q) sz += part[s][q][z][ij];
+      v = fma(c_trans[MODE][LC][k][z], sz, v);
+    }
+    const long long hi = mu > nu ? mu : nu, lo = mu > nu ? nu : mu;
+    const long long row = hi * (hi + 1) / 2 + lo;
+    out[mol.a_off + row * mol.naux + aux.func_off[sc] + k] = v;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // 2-centre metric (P | Q): same machinery with a zero-exponent partner at P
 // ---------------------------------------------------------------------------
 
@@ -403,8 +550,13 @@ __global__ void __launch_bounds__(128)
 
 template <int LA, int LB, int LC, bool SPH>
 static void launch3(const ClassLaunch& cl, const KernelArgs& k, cudaStream_t st) {
-  int3c_kernel<LA, LB, LC, SPH><<<cl.nblocks, Int3cCfg<LA, LB, LC, SPH>::THREADS, 0, st>>>(
-      k.orb, k.aux, k.xyz, k.mols, cl.pairs, cl.cms, cl.ncm, k.out);
+  if constexpr (use_root_parallel3c(LA, LB, LC, SPH)) {
+    int3c_rp_kernel<LA, LB, LC, SPH><<<cl.nblocks, rp_threads3c(LA, LB, LC, SPH), 0, st>>>(
+        k.orb, k.aux, k.xyz, k.mols, cl.pairs, cl.cms, cl.ncm, k.out);
+  } else {
+    int3c_kernel<LA, LB, LC, SPH><<<cl.nblocks, Int3cCfg<LA, LB, LC, SPH>::THREADS, 0, st>>>(
+        k.orb, k.aux, k.xyz, k.mols, cl.pairs, cl.cms, cl.ncm, k.out);
+  }
 }
 
 template <int LA, int LC, bool SPH>
