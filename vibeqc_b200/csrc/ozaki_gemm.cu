@@ -47,33 +47,50 @@ constexpr int BN = 64;
 constexpr int BKB = 128;  // K-block: 128 int8 = one 128-byte swizzle row = 4 MMA K-steps
 constexpr int kMaxSlices = 7;
 static_assert(BKB == 4 * 32, "the MMA issue loop is unrolled for four 32-byte K-steps per K-block");
-constexpr int kARing = 6;
+constexpr int kARing = 4;
 constexpr int kWRing = 2;
 constexpr int A_TILE = BM * BKB;              // 16 KB
 constexpr int B_TILE = BN * BKB;              // 8 KB
 constexpr int B_GROUP = kMaxSlices * B_TILE;  // 56 KB
 constexpr int kThreads = 224;  // A producer, MMA issuer, four epilogue warps, B producer
-constexpr int kStageLd = BN + 1;  // doubles per staged output row (padding against bank conflicts)
-static_assert(4 * 32 * kStageLd * 8 <= kARing * A_TILE, "epilogue staging fits in the A ring");
+constexpr int kStageCols = 32;                // columns per staging pass
+constexpr int kStageLd = kStageCols + 1;      // doubles per staged row (padding against bank conflicts)
+constexpr int STAGE_BYTES = 4 * 32 * kStageLd * 8;  // one 32-row block per epilogue warp
 constexpr int kTmemCols = 512;                // ns (<= 7) accumulators of BN columns
 
 struct OzCtrl {
-  uint64_t a_full[kARing], a_empty[kARing], b_full[kWRing], b_empty[kWRing], acc_full, drain;
+  uint64_t a_full[kARing], a_empty[kARing], b_full[kWRing], b_empty[kWRing], acc_full, tmem_empty,
+      drain;
   uint32_t tmem;
   int abort;
   int a_issued, a_consumed, b_issued, b_consumed;
 };
 
-constexpr int SMEM = kARing * A_TILE + kWRing * B_GROUP + 1024 + (int)sizeof(OzCtrl) + 64;
+constexpr int SMEM = kARing * A_TILE + kWRing * B_GROUP + STAGE_BYTES + 1024 + (int)sizeof(OzCtrl) + 64;
+static_assert(SMEM <= 227 * 1024, "shared memory per CTA");
 
 struct OzParams {
-  int m, n, k, ns, upper, ntn;
+  int m, n, k, ns, upper, ntn, ntm, ntiles;
   const int* a_exp;  // [nmol][m]
   const int* b_exp;  // [nmol][n]
   double* c;
   long long ldc, c_mol_stride;
   int* error;
 };
+
+// tile t -> (molecule, row tile, column tile), column tile fastest (CTAs that
+// run together share an A row block in L2)
+__device__ __forceinline__ void tile_coords(const OzParams& p, int t, int& z, int& tm, int& tn) {
+  tn = t % p.ntn;
+  const int r = t / p.ntn;
+  tm = r % p.ntm;
+  z = r / p.ntm;
+}
+
+__device__ __forceinline__ int tile_kblocks(const OzParams& p, int tn) {
+  const int kend = p.upper ? min(p.k, tn * BN + BN) : p.k;
+  return (kend + BKB - 1) / BKB;
+}
 
 __device__ __forceinline__ void oz_abort(OzCtrl* c, int* error, int code) {
   if (error) atomicExch(error, code);
@@ -133,6 +150,13 @@ __device__ __forceinline__ int slice_order(int j, int ns) { return (j & 1) ? ns 
 constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
                               ((uint32_t)(BM >> 4) << 24);
 
+
+// Persistent over output tiles: each CTA (one per SM: 512 TMEM columns)
+// takes tiles blockIdx.x, blockIdx.x + gridDim.x, ...  The producers run ahead
+// across tile boundaries, so the next tile's operands are in flight while the
+// epilogue drains the last one; the MMA issuer waits only until the epilogue
+// has read TMEM (tmem_empty), and the epilogue's FP64 scaling and stores
+// overlap the next tile's MMAs.
 __global__ void __launch_bounds__(kThreads, 1)
     ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                       OzParams p) {
@@ -141,21 +165,15 @@ __global__ void __launch_bounds__(kThreads, 1)
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
   uint8_t* abuf = smem;
   uint8_t* bbuf = smem + kARing * A_TILE;
-  OzCtrl* ctrl = reinterpret_cast<OzCtrl*>(bbuf + kWRing * B_GROUP);
+  double* stage_all = reinterpret_cast<double*>(bbuf + kWRing * B_GROUP);
+  OzCtrl* ctrl = reinterpret_cast<OzCtrl*>(reinterpret_cast<uint8_t*>(stage_all) + STAGE_BYTES);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int tn = blockIdx.x, tm = blockIdx.y, z = blockIdx.z;
-  const int m0 = tm * BM, n0 = tn * BN;
   const int ns = p.ns;
-  const int kend = p.upper ? min(p.k, n0 + BN) : p.k;
-  const int nkb = (kend + BKB - 1) / BKB;
 
   const uint32_t af0 = smem_u32(ctrl->a_full), ae0 = smem_u32(ctrl->a_empty);
   const uint32_t bf0 = smem_u32(ctrl->b_full), be0 = smem_u32(ctrl->b_empty);
-  const uint32_t accf = smem_u32(&ctrl->acc_full), drain = smem_u32(&ctrl->drain);
-  // the tile's column exponents, read by every epilogue thread (shared-memory
-  // broadcast instead of one global load per column and thread)
-  __shared__ int s_eb[BN];
-  if (tid < BN) s_eb[tid] = n0 + tid < p.n ? p.b_exp[(long long)z * p.n + n0 + tid] : 0;
+  const uint32_t accf = smem_u32(&ctrl->acc_full), tmem_empty = smem_u32(&ctrl->tmem_empty);
+  const uint32_t drain = smem_u32(&ctrl->drain);
   if (tid == 0) {
     for (int s = 0; s < kARing; ++s) {
       mbar_init(af0 + 8 * s, 1);
@@ -166,6 +184,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(be0 + 8 * s, 1);
     }
     mbar_init(accf, 1);
+    mbar_init(tmem_empty, 4);  // one arrival per epilogue warp
     mbar_init(drain, 1);
     ctrl->abort = 0;
     ctrl->a_issued = ctrl->a_consumed = ctrl->b_issued = ctrl->b_consumed = 0;
@@ -185,86 +204,118 @@ __global__ void __launch_bounds__(kThreads, 1)
   volatile int* ab = &ctrl->abort;
 
   if (warp == 6) {
-    if (lane == 0) {  // B-slice groups
-      for (int kb = 0; kb < nkb && !oz_aborted(ctrl); ++kb) {
-        const int ws = kb % kWRing;
-        if (kb >= kWRing && !mbar_wait(be0 + 8 * ws, ((kb / kWRing) - 1) & 1, ab)) {
-          oz_abort(ctrl, p.error, 41);
-          break;
-        }
-        mbar_expect_tx(bf0 + 8 * ws, ns * B_TILE);
-        for (int t = 0; t < ns; ++t)
-          tma_load_3d(smem_u32(bbuf + ws * B_GROUP + t * B_TILE), &tmB, kb * BKB, n0, z * ns + t,
-                      bf0 + 8 * ws);
-        *reinterpret_cast<volatile int*>(&ctrl->b_issued) = kb + 1;
-      }
-    }
-  } else if (warp == 0) {
-    if (lane == 0) {  // A-slice tiles
-      int ai = 0;
+    if (lane == 0) {  // B-slice groups, one per K-block of every tile
+      int gkb = 0;
       bool ok = true;
-      for (int kb = 0; kb < nkb && ok && !oz_aborted(ctrl); ++kb) {
-        for (int j = 0; j < ns; ++j, ++ai) {
-          const int as = ai % kARing;
-          if (ai >= kARing && !mbar_wait(ae0 + 8 * as, ((ai / kARing) - 1) & 1, ab)) {
-            oz_abort(ctrl, p.error, 42);
+      for (int t = blockIdx.x; t < p.ntiles && ok && !oz_aborted(ctrl); t += gridDim.x) {
+        int z, tm, tn;
+        tile_coords(p, t, z, tm, tn);
+        const int nkb = tile_kblocks(p, tn);
+        for (int kb = 0; kb < nkb; ++kb, ++gkb) {
+          const int ws = gkb % kWRing;
+          if (gkb >= kWRing && !mbar_wait(be0 + 8 * ws, ((gkb / kWRing) - 1) & 1, ab)) {
+            oz_abort(ctrl, p.error, 41);
             ok = false;
             break;
           }
-          mbar_expect_tx(af0 + 8 * as, A_TILE);
-          tma_load_3d(smem_u32(abuf + as * A_TILE), &tmA, kb * BKB, m0, z * ns + slice_order(j, ns),
-                      af0 + 8 * as);
-          *reinterpret_cast<volatile int*>(&ctrl->a_issued) = ai + 1;
+          mbar_expect_tx(bf0 + 8 * ws, ns * B_TILE);
+          for (int s = 0; s < ns; ++s)
+            tma_load_3d(smem_u32(bbuf + ws * B_GROUP + s * B_TILE), &tmB, kb * BKB, tn * BN,
+                        z * ns + s, bf0 + 8 * ws);
+          *reinterpret_cast<volatile int*>(&ctrl->b_issued) = gkb + 1;
+        }
+      }
+    }
+  } else if (warp == 0) {
+    if (lane == 0) {  // A-slice tiles in the interleaved slice order
+      int ai = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < p.ntiles && ok && !oz_aborted(ctrl); t += gridDim.x) {
+        int z, tm, tn;
+        tile_coords(p, t, z, tm, tn);
+        const int nkb = tile_kblocks(p, tn);
+        for (int kb = 0; kb < nkb && ok; ++kb) {
+          for (int j = 0; j < ns; ++j, ++ai) {
+            const int as = ai % kARing;
+            if (ai >= kARing && !mbar_wait(ae0 + 8 * as, ((ai / kARing) - 1) & 1, ab)) {
+              oz_abort(ctrl, p.error, 42);
+              ok = false;
+              break;
+            }
+            mbar_expect_tx(af0 + 8 * as, A_TILE);
+            tma_load_3d(smem_u32(abuf + as * A_TILE), &tmA, kb * BKB, tm * BM,
+                        z * ns + slice_order(j, ns), af0 + 8 * as);
+            *reinterpret_cast<volatile int*>(&ctrl->a_issued) = ai + 1;
+          }
         }
       }
     }
   } else if (warp == 1) {
     if (lane == 0) {  // MMA issuer
-      int ai = 0;
+      int ai = 0, gkb = 0, it = 0;
       bool ok = true;
-      for (int kb = 0; kb < nkb && ok && !oz_aborted(ctrl); ++kb) {
-        const int ws = kb % kWRing;
-        if (!mbar_wait(bf0 + 8 * ws, (kb / kWRing) & 1, ab)) {
-          oz_abort(ctrl, p.error, 43);
+      for (int t = blockIdx.x; t < p.ntiles && ok && !oz_aborted(ctrl); t += gridDim.x, ++it) {
+        int z, tm, tn;
+        tile_coords(p, t, z, tm, tn);
+        const int nkb = tile_kblocks(p, tn);
+        // the epilogue has read the previous tile's accumulators
+        if (it > 0 && !mbar_wait(tmem_empty, (it - 1) & 1, ab)) {
+          oz_abort(ctrl, p.error, 46);
           break;
         }
-        *reinterpret_cast<volatile int*>(&ctrl->b_consumed) = kb + 1;
-        const uint32_t bbase = smem_u32(bbuf + ws * B_GROUP);
-        for (int j = 0; j < ns; ++j, ++ai) {
-          const int s = slice_order(j, ns);
-          const int as = ai % kARing;
-          if (!mbar_wait(af0 + 8 * as, (ai / kARing) & 1, ab)) {
-            oz_abort(ctrl, p.error, 44);
+        fence_after_sync();
+        for (int kb = 0; kb < nkb && ok; ++kb, ++gkb) {
+          const int ws = gkb % kWRing;
+          if (!mbar_wait(bf0 + 8 * ws, (gkb / kWRing) & 1, ab)) {
+            oz_abort(ctrl, p.error, 43);
             ok = false;
             break;
           }
-          *reinterpret_cast<volatile int*>(&ctrl->a_consumed) = ai + 1;
-          fence_after_sync();
-          // slices are 0-based here: pair (s, t) with s + t <= ns - 1 feeds
-          // accumulator g = s + t (weight 2^-7(g+2)); four 32-byte K-steps per
-          // K-block (measured faster than a fully unrolled form)
-          const uint32_t abase = smem_u32(abuf + as * A_TILE);
-          for (int t = 0; t + s < ns; ++t) {
-            const uint32_t dt = tmem + (uint32_t)((s + t) * BN);
+          *reinterpret_cast<volatile int*>(&ctrl->b_consumed) = gkb + 1;
+          const uint32_t bbase = smem_u32(bbuf + ws * B_GROUP);
+          for (int j = 0; j < ns; ++j, ++ai) {
+            const int s = slice_order(j, ns);
+            const int as = ai % kARing;
+            if (!mbar_wait(af0 + 8 * as, (ai / kARing) & 1, ab)) {
+              oz_abort(ctrl, p.error, 44);
+              ok = false;
+              break;
+            }
+            *reinterpret_cast<volatile int*>(&ctrl->a_consumed) = ai + 1;
+            fence_after_sync();
+            // slices are 0-based here: pair (s, t) with s + t <= ns - 1 feeds
+            // accumulator g = s + t (weight 2^-7(g+2)); slice 0 comes first in
+            // the issue order, so its first K-step initialises every accumulator
+            const uint32_t abase = smem_u32(abuf + as * A_TILE);
+            for (int tt = 0; tt + s < ns; ++tt) {
+              const uint32_t dt = tmem + (uint32_t)((s + tt) * BN);
 #pragma unroll
-            for (int kk = 0; kk < BKB / 32; ++kk)
-              mma_i8(dt, smem_desc(abase + kk * 32), smem_desc(bbase + t * B_TILE + kk * 32),
-                     kIdescI8, (kb == 0 && s == 0 && kk == 0) ? 0u : 1u);
+              for (int kk = 0; kk < BKB / 32; ++kk)
+                mma_i8(dt, smem_desc(abase + kk * 32), smem_desc(bbase + tt * B_TILE + kk * 32),
+                       kIdescI8, (kb == 0 && s == 0 && kk == 0) ? 0u : 1u);
+            }
+            mma_commit(ae0 + 8 * as);
           }
-          mma_commit(ae0 + 8 * as);
+          if (ok) mma_commit(be0 + 8 * ws);
         }
-        if (ok) mma_commit(be0 + 8 * ws);
+        if (ok) mma_commit(accf);
       }
-      if (ok && !oz_aborted(ctrl)) mma_commit(accf);
       mma_commit(drain);  // arrives once every MMA issued above has completed
     }
   } else {  // epilogue warps 2..5: TMEM lane quarter (warp & 3)
     const int q = warp & 3;
-    // the whole tile's MMAs run before this wait ends: poll with back-off
-    const bool ok = __all_sync(0xffffffffu, mbar_wait_backoff(accf, 0, ab, kWaitNs, 256));
-    if (!ok) {
-      if (lane == 0) oz_abort(ctrl, p.error, 45);
-    } else {
+    double* stage = stage_all + (size_t)(warp - 2) * 32 * kStageLd;
+    int it = 0;
+    for (int t = blockIdx.x; t < p.ntiles; t += gridDim.x, ++it) {
+      int z, tm, tn;
+      tile_coords(p, t, z, tm, tn);
+      const int m0 = tm * BM, n0 = tn * BN;
+      // the tile's MMAs run before this wait ends: poll with back-off
+      const bool ok = __all_sync(0xffffffffu, mbar_wait_backoff(accf, it & 1, ab, kWaitNs, 256));
+      if (!ok) {
+        if (lane == 0) oz_abort(ctrl, p.error, 45);
+        break;
+      }
       fence_after_sync();
       const int row = m0 + q * 32 + lane;
       double acc[BN];
@@ -277,33 +328,46 @@ __global__ void __launch_bounds__(kThreads, 1)
         tmem_ld32_i32_nowait(ta, v);
         tmem_ld32_i32_nowait(ta + 32, v + 32);
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (g == ns - 1) {
+          // every accumulator of this tile is in registers: the MMA issuer may
+          // start the next tile
+          fence_before_sync();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(tmem_empty);
+        }
 #pragma unroll
         for (int c = 0; c < BN; ++c) acc[c] = fma((double)v[c], scale, acc[c]);
       }
-      // scale by 2^(ea + eb) in one step (no intermediate underflow), stage the
-      // warp's 32 rows in the idle A ring, then store whole rows.  For a normal
-      // power of two the product with 2^e (built from its exponent bits) is
-      // exactly ldexp (one rounding, only when the result is subnormal);
-      // exponents outside the normal range take ldexp itself.
+      // scale by 2^(ea + eb) in one step (no intermediate underflow): for a
+      // normal power of two the product with 2^e built from its exponent bits
+      // is exactly ldexp (one rounding, only for a subnormal result); other
+      // exponents take ldexp itself.  Lane c holds the exponents of columns
+      // c and c + 32; each 32-column half is staged and stored as whole rows.
       const int ea = row < p.m ? p.a_exp[(long long)z * p.m + row] : 0;
-      double* stage = reinterpret_cast<double*>(abuf) + (size_t)(warp - 2) * 32 * kStageLd;
+      const int* eb = p.b_exp + (long long)z * p.n;
+      const int eb_lo = n0 + lane < p.n ? eb[n0 + lane] : 0;
+      const int eb_hi = n0 + 32 + lane < p.n ? eb[n0 + 32 + lane] : 0;
 #pragma unroll
-      for (int c = 0; c < BN; ++c) {
-        const int e = ea + s_eb[c];
-        double v = acc[c];
-        if (e >= -1022 && e <= 1023)
-          v *= __longlong_as_double((long long)(e + 1023) << 52);
-        else
-          v = ldexp(v, e);
-        stage[lane * kStageLd + c] = n0 + c < p.n ? v : 0.0;
-      }
-      __syncwarp();
-      const int rbase = m0 + q * 32;
-      for (int r = 0; r < 32; ++r) {
-        if (rbase + r >= p.m) break;
-        double* out = p.c + (long long)z * p.c_mol_stride + (long long)(rbase + r) * p.ldc + n0;
-        if (n0 + lane < p.n) out[lane] = stage[r * kStageLd + lane];
-        if (n0 + 32 + lane < p.n) out[32 + lane] = stage[r * kStageLd + 32 + lane];
+      for (int h = 0; h < 2; ++h) {
+#pragma unroll
+        for (int c = 0; c < kStageCols; ++c) {
+          const int e = ea + __shfl_sync(0xffffffffu, h ? eb_hi : eb_lo, c);
+          double x = acc[h * kStageCols + c];
+          if (e >= -1022 && e <= 1023)
+            x *= __longlong_as_double((long long)(e + 1023) << 52);
+          else
+            x = ldexp(x, e);
+          stage[lane * kStageLd + c] = n0 + h * kStageCols + c < p.n ? x : 0.0;
+        }
+        __syncwarp();
+        const int rbase = m0 + q * 32;
+        for (int r = 0; r < 32; ++r) {
+          if (rbase + r >= p.m) break;
+          double* out = p.c + (long long)z * p.c_mol_stride + (long long)(rbase + r) * p.ldc + n0 +
+                        h * kStageCols;
+          if (n0 + h * kStageCols + lane < p.n) out[lane] = stage[r * kStageLd + lane];
+        }
+        __syncwarp();
       }
     }
     fence_before_sync();
@@ -422,6 +486,10 @@ extern "C" int vqc_ozaki_gemm(const int8_t* a_slices, const int32_t* a_exps, int
   p.ns = nslices;
   p.upper = upper ? 1 : 0;
   p.ntn = (n + oz::BN - 1) / oz::BN;
+  p.ntm = (int)((m + oz::BM - 1) / oz::BM);
+  const long long ntiles = (long long)p.ntn * p.ntm * nmol;
+  if (ntiles > 0x7fffffffLL) return fail(VQC_STATUS_INVALID_ARGUMENT, "ozaki_gemm: too many tiles");
+  p.ntiles = (int)ntiles;
   p.a_exp = a_exps;
   p.b_exp = b_exps;
   p.c = c;
@@ -431,8 +499,9 @@ extern "C" int vqc_ozaki_gemm(const int8_t* a_slices, const int32_t* a_exps, int
   cudaError_t e = cudaFuncSetAttribute(oz::ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        oz::SMEM);
   if (e != cudaSuccess) return cuda_status(e, "ozaki smem attribute");
-  dim3 grid(p.ntn, (unsigned)((m + oz::BM - 1) / oz::BM), nmol);
-  oz::ozaki_gemm_kernel<<<grid, oz::kThreads, oz::SMEM, (cudaStream_t)stream>>>(ta, tb, p);
+  const int sms = vqc::tc::sm_count();
+  const int ctas = p.ntiles < sms ? p.ntiles : sms;  // persistent: one CTA per SM
+  oz::ozaki_gemm_kernel<<<ctas, oz::kThreads, oz::SMEM, (cudaStream_t)stream>>>(ta, tb, p);
   count_launch();
   return cuda_status(cudaGetLastError(), "ozaki_gemm");
 }
