@@ -47,15 +47,12 @@ constexpr int BN = 64;
 constexpr int BKB = 128;  // K-block: 128 int8 = one 128-byte swizzle row = 4 MMA K-steps
 constexpr int kMaxSlices = 7;
 static_assert(BKB == 4 * 32, "the MMA issue loop is unrolled for four 32-byte K-steps per K-block");
-constexpr int kARing = 4;
+constexpr int kARing = 6;
 constexpr int kWRing = 2;
 constexpr int A_TILE = BM * BKB;              // 16 KB
 constexpr int B_TILE = BN * BKB;              // 8 KB
 constexpr int B_GROUP = kMaxSlices * B_TILE;  // 56 KB
 constexpr int kThreads = 224;  // A producer, MMA issuer, four epilogue warps, B producer
-constexpr int kStageCols = 32;                // columns per staging pass
-constexpr int kStageLd = kStageCols + 1;      // doubles per staged row (padding against bank conflicts)
-constexpr int STAGE_BYTES = 4 * 32 * kStageLd * 8;  // one 32-row block per epilogue warp
 constexpr int kTmemCols = 512;                // ns (<= 7) accumulators of BN columns
 
 struct OzCtrl {
@@ -66,7 +63,7 @@ struct OzCtrl {
   int a_issued, a_consumed, b_issued, b_consumed;
 };
 
-constexpr int SMEM = kARing * A_TILE + kWRing * B_GROUP + STAGE_BYTES + 1024 + (int)sizeof(OzCtrl) + 64;
+constexpr int SMEM = kARing * A_TILE + kWRing * B_GROUP + 1024 + (int)sizeof(OzCtrl) + 64;
 static_assert(SMEM <= 227 * 1024, "shared memory per CTA");
 
 struct OzParams {
@@ -165,8 +162,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
   uint8_t* abuf = smem;
   uint8_t* bbuf = smem + kARing * A_TILE;
-  double* stage_all = reinterpret_cast<double*>(bbuf + kWRing * B_GROUP);
-  OzCtrl* ctrl = reinterpret_cast<OzCtrl*>(reinterpret_cast<uint8_t*>(stage_all) + STAGE_BYTES);
+  OzCtrl* ctrl = reinterpret_cast<OzCtrl*>(bbuf + kWRing * B_GROUP);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int ns = p.ns;
 
@@ -272,7 +268,9 @@ __global__ void __launch_bounds__(kThreads, 1)
             break;
           }
           *reinterpret_cast<volatile int*>(&ctrl->b_consumed) = gkb + 1;
-          const uint32_t bbase = smem_u32(bbuf + ws * B_GROUP);
+          // descriptors advance by (byte offset >> 4) in their address field
+          // (shared-memory addresses < 256 KB never carry out of it)
+          const uint64_t bdesc0 = smem_desc(smem_u32(bbuf + ws * B_GROUP));
           for (int j = 0; j < ns; ++j, ++ai) {
             const int s = slice_order(j, ns);
             const int as = ai % kARing;
@@ -286,13 +284,15 @@ __global__ void __launch_bounds__(kThreads, 1)
             // slices are 0-based here: pair (s, t) with s + t <= ns - 1 feeds
             // accumulator g = s + t (weight 2^-7(g+2)); slice 0 comes first in
             // the issue order, so its first K-step initialises every accumulator
-            const uint32_t abase = smem_u32(abuf + as * A_TILE);
-            for (int tt = 0; tt + s < ns; ++tt) {
-              const uint32_t dt = tmem + (uint32_t)((s + tt) * BN);
-#pragma unroll
-              for (int kk = 0; kk < BKB / 32; ++kk)
-                mma_i8(dt, smem_desc(abase + kk * 32), smem_desc(bbase + tt * B_TILE + kk * 32),
-                       kIdescI8, (kb == 0 && s == 0 && kk == 0) ? 0u : 1u);
+            const uint64_t adesc0 = smem_desc(smem_u32(abuf + as * A_TILE));
+            const uint32_t first = (kb == 0 && s == 0) ? 0u : 1u;
+            uint32_t dt = tmem + (uint32_t)(s * BN);
+            uint64_t bdesc = bdesc0;
+            for (int tt = 0; tt + s < ns; ++tt, dt += BN, bdesc += B_TILE >> 4) {
+              mma_i8(dt, adesc0, bdesc, kIdescI8, first);
+              mma_i8(dt, adesc0 + 2, bdesc + 2, kIdescI8, 1u);
+              mma_i8(dt, adesc0 + 4, bdesc + 4, kIdescI8, 1u);
+              mma_i8(dt, adesc0 + 6, bdesc + 6, kIdescI8, 1u);
             }
             mma_commit(ae0 + 8 * as);
           }
@@ -304,7 +304,6 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   } else {  // epilogue warps 2..5: TMEM lane quarter (warp & 3)
     const int q = warp & 3;
-    double* stage = stage_all + (size_t)(warp - 2) * 32 * kStageLd;
     int it = 0;
     for (int t = blockIdx.x; t < p.ntiles; t += gridDim.x, ++it) {
       int z, tm, tn;
@@ -342,32 +341,35 @@ __global__ void __launch_bounds__(kThreads, 1)
       // normal power of two the product with 2^e built from its exponent bits
       // is exactly ldexp (one rounding, only for a subnormal result); other
       // exponents take ldexp itself.  Lane c holds the exponents of columns
-      // c and c + 32; each 32-column half is staged and stored as whole rows.
+      // c and c + 32.  Each thread stores its own row in 16-byte pieces (the
+      // shared memory holds the operand rings).
       const int ea = row < p.m ? p.a_exp[(long long)z * p.m + row] : 0;
       const int* eb = p.b_exp + (long long)z * p.n;
       const int eb_lo = n0 + lane < p.n ? eb[n0 + lane] : 0;
       const int eb_hi = n0 + 32 + lane < p.n ? eb[n0 + 32 + lane] : 0;
+      double* out = p.c + (long long)z * p.c_mol_stride + (long long)row * p.ldc + n0;
+      const bool full_row = row < p.m && n0 + BN <= p.n &&
+                            ((reinterpret_cast<uintptr_t>(out) & 15) == 0);
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
+      for (int c = 0; c < BN; c += 2) {
+        double x2[2];
 #pragma unroll
-        for (int c = 0; c < kStageCols; ++c) {
-          const int e = ea + __shfl_sync(0xffffffffu, h ? eb_hi : eb_lo, c);
-          double x = acc[h * kStageCols + c];
-          if (e >= -1022 && e <= 1023)
-            x *= __longlong_as_double((long long)(e + 1023) << 52);
+        for (int e = 0; e < 2; ++e) {
+          const int col = c + e;
+          const int ex = ea + __shfl_sync(0xffffffffu, col < 32 ? eb_lo : eb_hi, col & 31);
+          double x = acc[col];
+          if (ex >= -1022 && ex <= 1023)
+            x *= __longlong_as_double((long long)(ex + 1023) << 52);
           else
-            x = ldexp(x, e);
-          stage[lane * kStageLd + c] = n0 + h * kStageCols + c < p.n ? x : 0.0;
+            x = ldexp(x, ex);
+          x2[e] = x;
         }
-        __syncwarp();
-        const int rbase = m0 + q * 32;
-        for (int r = 0; r < 32; ++r) {
-          if (rbase + r >= p.m) break;
-          double* out = p.c + (long long)z * p.c_mol_stride + (long long)(rbase + r) * p.ldc + n0 +
-                        h * kStageCols;
-          if (n0 + h * kStageCols + lane < p.n) out[lane] = stage[r * kStageLd + lane];
+        if (full_row) {
+          *reinterpret_cast<double2*>(out + c) = make_double2(x2[0], x2[1]);
+        } else if (row < p.m) {
+          if (n0 + c < p.n) out[c] = x2[0];
+          if (n0 + c + 1 < p.n) out[c + 1] = x2[1];
         }
-        __syncwarp();
       }
     }
     fence_before_sync();
