@@ -122,6 +122,18 @@ int vqc_plan_molecule(const vqc_plan* plan, int32_t index, vqc_molecule_info* in
 int vqc_int1e(vqc_plan* plan, const double* xyz, double* s, double* t, double* v, void* stream);
 int vqc_int2c(vqc_plan* plan, const double* xyz, double* metric, void* stream);
 int vqc_int3c(vqc_plan* plan, const double* xyz, double* a_packed, void* stream);
+/* Bounded 3-centre row tiles: the packed rows of one molecule whose larger AO
+ * index mu lies in the functions of its orbital shells [shell_begin,
+ * shell_end) (shell indices counted within the molecule), i.e. rows
+ * mu(mu+1)/2 + nu - f0(f0+1)/2 for f0 <= mu < f1, nu <= mu, where f0 / f1 are
+ * the first functions of shell_begin / shell_end: (f1(f1+1)/2 - f0(f0+1)/2) x
+ * naux doubles, the same values vqc_int3c writes there.  Replaces the
+ * reference's bounded DF integral source tiles
+ * (src/scf/cuda/df_source.cpp:347-372, generate_cuda_density_fitting_raw_tile)
+ * for recompute under a memory bound.  Calls on one plan are stream-ordered:
+ * they share a small work table inside the plan. */
+int vqc_int3c_rows(vqc_plan* plan, const double* xyz, int32_t mol, int32_t shell_begin,
+                   int32_t shell_end, double* rows, void* stream);
 
 /*
  * Gradient contractions (accumulate into grad[natom][3]; the caller zeroes it).

@@ -104,6 +104,8 @@ _SIGNATURES = {
     "vqc_int1e": ([_P, _P, _P, _P, _P, _P], ctypes.c_int),
     "vqc_int2c": ([_P, _P, _P, _P], ctypes.c_int),
     "vqc_int3c": ([_P, _P, _P, _P], ctypes.c_int),
+    "vqc_int3c_rows": ([_P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _P, _P],
+                       ctypes.c_int),
     "vqc_grad3c": ([_P, _P, _P, _P, _P], ctypes.c_int),
     "vqc_grad2c": ([_P, _P, _P, _P, _P], ctypes.c_int),
     "vqc_grad1e": ([_P, _P, _P, _P, _P, _P], ctypes.c_int),

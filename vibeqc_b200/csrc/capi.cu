@@ -97,6 +97,7 @@ static int build_shells(const int32_t* l, const int32_t* atom, const int32_t* np
 int Plan::build(const vqc_batch_desc& d) {
   nmol = d.nmol;
   sph = d.spherical != 0;
+  mol_shell_off.assign(d.mol_shell_offset, d.mol_shell_offset + d.nmol + 1);
   natom = d.mol_atom_offset[nmol];
   int st = build_shells(d.shell_l, d.shell_atom, d.shell_nprim, d.shell_prim_off, d.nprim,
                         d.mol_shell_offset, d.mol_atom_offset, nmol, sph, orb_h, nao, "orbital");
@@ -231,6 +232,11 @@ int Plan::build(const vqc_batch_desc& d) {
         if (qcnt[c][m]) cm2.push_back(ClassMol{m, qbeg[c][m], 0, 0, qcnt[c][m], 0});
       if ((st = add_class(cls2c, la, 0, lb, dpairs2[c], cm2, slots2c(lb)))) return st;
     }
+  // scratch of the bounded row tiles: one molecule view, one entry per class
+  std::vector<DevMol> view(1);
+  if ((st = upload(owned, view, &dtile_mol))) return st;
+  std::vector<ClassMol> tcms(std::max<size_t>(1, cls3c.size()));
+  if ((st = upload(owned, tcms, &dtile_cms))) return st;
   return VQC_STATUS_SUCCESS;
 }
 
@@ -363,6 +369,65 @@ int vqc_int3c(vqc_plan* plan, const double* xyz, double* a_packed, void* stream)
   k.xyz = xyz;
   k.out = a_packed;
   return run_classes(p, p->cls3c, dispatch_int3c, k, (cudaStream_t)stream, "int3c");
+  VQC_GUARD_END
+}
+
+int vqc_int3c_rows(vqc_plan* plan, const double* xyz, int32_t mol, int32_t shell_begin,
+                   int32_t shell_end, double* rows, void* stream) {
+  VQC_GUARD_BEGIN
+  if (!plan || !xyz || !rows) return fail(VQC_STATUS_INVALID_ARGUMENT, "null argument");
+  Plan* p = reinterpret_cast<Plan*>(plan);
+  if (mol < 0 || mol >= p->nmol) return fail(VQC_STATUS_INVALID_ARGUMENT, "int3c_rows: molecule index");
+  const int s0 = p->mol_shell_off[mol], s1 = p->mol_shell_off[mol + 1];
+  if (shell_begin < 0 || shell_end <= shell_begin || s0 + shell_end > s1)
+    return fail(VQC_STATUS_INVALID_ARGUMENT, "int3c_rows: shell range outside the molecule");
+  const int a0 = s0 + shell_begin, a1 = s0 + shell_end;
+  const long long f0 = p->orb_h.func_off[a0];
+  const long long naux = p->mols_h[mol].naux;
+  // the molecule seen through the tile: packed rows counted from the tile's first row
+  DevMol view = p->mols_h[mol];
+  view.a_off = -(f0 * (f0 + 1) / 2) * naux;
+  // pairs (a, b <= a) of a class are listed in order of a, so the tile's pairs
+  // (a in [a0, a1)) are one contiguous run per class: count the pairs before it
+  auto class_of = [&](int a, int b) {
+    const int la = p->orb_h.l[a], lb = p->orb_h.l[b];
+    return std::max(la, lb) * 4 + std::min(la, lb);
+  };
+  int before[16] = {0}, inside[16] = {0};
+  for (int a = s0; a < a1; ++a)
+    for (int b = s0; b <= a; ++b) (a < a0 ? before : inside)[class_of(a, b)]++;
+  std::vector<ClassMol> cms;
+  std::vector<ClassLaunch> launches;
+  for (size_t i = 0; i < p->cls3c.size(); ++i) {
+    const ClassLaunch& cl = p->cls3c[i];
+    const int c = cl.la * 4 + cl.lb;
+    if (!inside[c]) continue;
+    const ClassMol* cm = nullptr;
+    for (const ClassMol& e : p->cls3c_host[i])
+      if (e.mol == mol) cm = &e;
+    if (!cm) continue;  // no auxiliary shell of this class's l in the molecule
+    const long long tri = (long long)inside[c] * cm->naux;
+    const int per = slots3c(cl.la, cl.lb, cl.lc, p->sph);
+    ClassLaunch tl = cl;
+    tl.cms = p->dtile_cms + cms.size();
+    tl.ncm = 1;
+    tl.nblocks = (int)((tri + per - 1) / per);
+    cms.push_back(ClassMol{0, cm->pair_begin + before[c], cm->aux_begin, cm->naux, (int)tri, 0});
+    launches.push_back(tl);
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e;
+  if ((e = cudaMemcpyAsync(p->dtile_mol, &view, sizeof(DevMol), cudaMemcpyHostToDevice, st)))
+    return cuda_status(e, "int3c_rows view upload");
+  if (!cms.empty() &&
+      (e = cudaMemcpyAsync(p->dtile_cms, cms.data(), cms.size() * sizeof(ClassMol),
+                           cudaMemcpyHostToDevice, st)))
+    return cuda_status(e, "int3c_rows work upload");
+  KernelArgs k = p->args;
+  k.xyz = xyz;
+  k.out = rows;
+  k.mols = p->dtile_mol;
+  return run_classes(p, launches, dispatch_int3c, k, st, "int3c_rows");
   VQC_GUARD_END
 }
 

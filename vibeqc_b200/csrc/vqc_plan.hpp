@@ -41,6 +41,12 @@ struct Plan {
   // host copies of the per-molecule work entries of each cls3c launch (the
   // tiled gradient entry re-slices them by auxiliary shell range)
   std::vector<std::vector<ClassMol>> cls3c_host;
+  // orbital shell range of every molecule (global shell indices), and a
+  // device scratch (one molecule view + one work entry per 3-centre class)
+  // for the bounded row tiles of vqc_int3c_rows
+  std::vector<int> mol_shell_off;
+  DevMol* dtile_mol = nullptr;
+  ClassMol* dtile_cms = nullptr;
 
   int build(const vqc_batch_desc& d);
   ~Plan();
