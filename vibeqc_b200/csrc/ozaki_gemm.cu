@@ -52,7 +52,10 @@ constexpr int kWRing = 2;
 constexpr int A_TILE = BM * BKB;              // 16 KB
 constexpr int B_TILE = BN * BKB;              // 8 KB
 constexpr int B_GROUP = kMaxSlices * B_TILE;  // 56 KB
-constexpr int kThreads = 224;  // A producer, MMA issuer, four epilogue warps, B producer
+// MMA issuers: the int8 MMA costs ~150 cycles of issue per instruction whatever its N, so
+// two issuing warps (accumulators split by parity) keep more of them in flight
+constexpr int kIssuers = 2;
+constexpr int kThreads = 32 * (7 + kIssuers - 1);  // A producer, issuer 0, 4 epilogue, B producer, issuer 1
 constexpr int kTmemCols = 512;                // ns (<= 7) accumulators of BN columns
 
 struct OzCtrl {
@@ -173,15 +176,15 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (tid == 0) {
     for (int s = 0; s < kARing; ++s) {
       mbar_init(af0 + 8 * s, 1);
-      mbar_init(ae0 + 8 * s, 1);
+      mbar_init(ae0 + 8 * s, kIssuers);
     }
     for (int s = 0; s < kWRing; ++s) {
       mbar_init(bf0 + 8 * s, 1);
-      mbar_init(be0 + 8 * s, 1);
+      mbar_init(be0 + 8 * s, kIssuers);
     }
-    mbar_init(accf, 1);
+    mbar_init(accf, kIssuers);
     mbar_init(tmem_empty, 4);  // one arrival per epilogue warp
-    mbar_init(drain, 1);
+    mbar_init(drain, kIssuers);
     ctrl->abort = 0;
     ctrl->a_issued = ctrl->a_consumed = ctrl->b_issued = ctrl->b_consumed = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -246,7 +249,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
       }
     }
-  } else if (warp == 1) {
+  } else if (warp == 1 || warp >= 7) {
+    const int me = warp == 1 ? 0 : warp - 6;  // issuer index: accumulators g with g % kIssuers == me
     if (lane == 0) {  // MMA issuer
       int ai = 0, gkb = 0, it = 0;
       bool ok = true;
@@ -267,7 +271,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             ok = false;
             break;
           }
-          *reinterpret_cast<volatile int*>(&ctrl->b_consumed) = gkb + 1;
+          if (me == 0) *reinterpret_cast<volatile int*>(&ctrl->b_consumed) = gkb + 1;
           // descriptors advance by (byte offset >> 4) in their address field
           // (shared-memory addresses < 256 KB never carry out of it)
           const uint64_t bdesc0 = smem_desc(smem_u32(bbuf + ws * B_GROUP));
@@ -279,7 +283,7 @@ __global__ void __launch_bounds__(kThreads, 1)
               ok = false;
               break;
             }
-            *reinterpret_cast<volatile int*>(&ctrl->a_consumed) = ai + 1;
+            if (me == 0) *reinterpret_cast<volatile int*>(&ctrl->a_consumed) = ai + 1;
             fence_after_sync();
             // slices are 0-based here: pair (s, t) with s + t <= ns - 1 feeds
             // accumulator g = s + t (weight 2^-7(g+2)); slice 0 comes first in
@@ -289,6 +293,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             uint32_t dt = tmem + (uint32_t)(s * BN);
             uint64_t bdesc = bdesc0;
             for (int tt = 0; tt + s < ns; ++tt, dt += BN, bdesc += B_TILE >> 4) {
+              if ((s + tt) % kIssuers != me) continue;
               mma_i8(dt, adesc0, bdesc, kIdescI8, first);
               mma_i8(dt, adesc0 + 2, bdesc + 2, kIdescI8, 1u);
               mma_i8(dt, adesc0 + 4, bdesc + 4, kIdescI8, 1u);
@@ -302,7 +307,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
       mma_commit(drain);  // arrives once every MMA issued above has completed
     }
-  } else {  // epilogue warps 2..5: TMEM lane quarter (warp & 3)
+  } else if (warp >= 2 && warp <= 5) {  // epilogue warps 2..5: TMEM lane quarter (warp & 3)
     const int q = warp & 3;
     int it = 0;
     for (int t = blockIdx.x; t < p.ntiles; t += gridDim.x, ++it) {

@@ -34,20 +34,27 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
                : "memory");
 }
 
-// bounded wait; false on timeout (budget_ns of %globaltimer) or when *abort is set
+__device__ __forceinline__ uint32_t mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred P;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, P;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok;
+}
+
+// bounded wait; false on timeout (budget_ns of %globaltimer) or when *abort is set.
+// The barrier is tried once before the clock is read: on the common path (the
+// phase has already completed) the wait costs one try_wait, not a timer read.
 __device__ __forceinline__ bool mbar_wait_for(uint32_t bar, uint32_t parity, volatile int* abort,
                                               unsigned long long budget_ns) {
+  if (mbar_try(bar, parity)) return true;
   const unsigned long long t0 = globaltimer();
   while (true) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred P;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
-        "selp.b32 %0, 1, 0, P;\n\t}"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    if (ok) return true;
+    if (mbar_try(bar, parity)) return true;
     if (*abort) return false;
     if (globaltimer() - t0 > budget_ns) return false;
   }
@@ -57,17 +64,10 @@ __device__ __forceinline__ bool mbar_wait_for(uint32_t bar, uint32_t parity, vol
 // critical path (they would otherwise steal issue slots from the warps that are)
 __device__ __forceinline__ bool mbar_wait_backoff(uint32_t bar, uint32_t parity, volatile int* abort,
                                                   unsigned long long budget_ns, unsigned sleep_ns) {
+  if (mbar_try(bar, parity)) return true;
   const unsigned long long t0 = globaltimer();
   while (true) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred P;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
-        "selp.b32 %0, 1, 0, P;\n\t}"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    if (ok) return true;
+    if (mbar_try(bar, parity)) return true;
     if (*abort) return false;
     if (globaltimer() - t0 > budget_ns) return false;
     __nanosleep(sleep_ns);
