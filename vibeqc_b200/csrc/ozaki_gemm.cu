@@ -111,6 +111,14 @@ __device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t
       : "memory");
 }
 
+// accumulate into D (no predicate to set up)
+__device__ __forceinline__ void mma_i8_acc(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                           uint32_t idesc) {
+  asm volatile("tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, 1;" ::"r"(tmem_d), "l"(adesc),
+               "l"(bdesc), "r"(idesc)
+               : "memory");
+}
+
 // 32 consecutive columns of a lane quarter, without waiting (tcgen05.wait::ld
 // follows once all loads of an accumulator are in flight)
 __device__ __forceinline__ void tmem_ld32_i32_nowait(uint32_t taddr, int* v) {
@@ -294,10 +302,11 @@ __global__ void __launch_bounds__(kThreads, 1)
             uint64_t bdesc = bdesc0;
             for (int tt = 0; tt + s < ns; ++tt, dt += BN, bdesc += B_TILE >> 4) {
               if ((s + tt) % kIssuers != me) continue;
-              mma_i8(dt, adesc0, bdesc, kIdescI8, first);
-              mma_i8(dt, adesc0 + 2, bdesc + 2, kIdescI8, 1u);
-              mma_i8(dt, adesc0 + 4, bdesc + 4, kIdescI8, 1u);
-              mma_i8(dt, adesc0 + 6, bdesc + 6, kIdescI8, 1u);
+              if (first) mma_i8_acc(dt, adesc0, bdesc, kIdescI8);
+              else mma_i8(dt, adesc0, bdesc, kIdescI8, 0u);
+              mma_i8_acc(dt, adesc0 + 2, bdesc + 2, kIdescI8);
+              mma_i8_acc(dt, adesc0 + 4, bdesc + 4, kIdescI8);
+              mma_i8_acc(dt, adesc0 + 6, bdesc + 6, kIdescI8);
             }
             mma_commit(ae0 + 8 * as);
           }

@@ -62,6 +62,14 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64
       : "memory");
 }
 
+// accumulate into D (no predicate to set up)
+__device__ __forceinline__ void mma_tf32_acc(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                             uint32_t idesc) {
+  asm volatile("tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, 1;" ::"r"(tmem_d), "l"(adesc),
+               "l"(bdesc), "r"(idesc)
+               : "memory");
+}
+
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   uint32_t r[16];
   asm volatile(
@@ -343,15 +351,19 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
             break;
           }
           fence_after_sync();
-          const uint32_t ahi = smem_u32(stage(s)), alo = ahi + C::A_BYTES;
-          const uint32_t chi = ahi + 2 * C::A_BYTES, clo = chi + C::C_BYTES;
+          // descriptors advance by (byte offset >> 4) in their address field
+          const uint32_t ahi = smem_u32(stage(s));
+          const uint64_t dahi = smem_desc(ahi), dalo = smem_desc(ahi + C::A_BYTES);
+          const uint64_t dchi = smem_desc(ahi + 2 * C::A_BYTES);
+          const uint64_t dclo = smem_desc(ahi + 2 * C::A_BYTES + C::C_BYTES);
+          const uint32_t acc0 = kb == 0 ? 0u : 1u;
 #pragma unroll
           for (int kk = 0; kk < BK / 8; ++kk) {
-            const uint32_t off = kk * 32;
-            mma_tf32(dt, smem_desc(alo + off), smem_desc(chi + off), idesc,
-                     (kb == 0 && kk == 0) ? 0u : 1u);
-            mma_tf32(dt, smem_desc(ahi + off), smem_desc(clo + off), idesc, 1u);
-            mma_tf32(dt, smem_desc(ahi + off), smem_desc(chi + off), idesc, 1u);
+            const uint64_t off = (uint64_t)kk * 2;  // 32 bytes per K-step
+            if (kk == 0) mma_tf32(dt, dalo + off, dchi + off, idesc, acc0);
+            else mma_tf32_acc(dt, dalo + off, dchi + off, idesc);
+            mma_tf32_acc(dt, dahi + off, dclo + off, idesc);
+            mma_tf32_acc(dt, dahi + off, dchi + off, idesc);
           }
           mma_commit(empty0 + 8 * s);
           *reinterpret_cast<volatile int*>(&ctrl->commits) = g + 1;
@@ -574,15 +586,18 @@ __global__ void __launch_bounds__(kGramThreads, 1)
           }
           *reinterpret_cast<volatile int*>(&ctrl->consumed) = i + 1;
           fence_after_sync();
-          const uint32_t ahi = smem_u32(stage(s)), alo = ahi + C::TILE;
-          const uint32_t bhi = ahi + 2 * C::TILE, blo = ahi + 3 * C::TILE;
+          // descriptors advance by (byte offset >> 4) in their address field
+          const uint32_t ahi = smem_u32(stage(s));
+          const uint64_t dahi = smem_desc(ahi), dalo = smem_desc(ahi + C::TILE);
+          const uint64_t dbhi = smem_desc(ahi + 2 * C::TILE), dblo = smem_desc(ahi + 3 * C::TILE);
+          const uint32_t acc0 = i == first ? 0u : 1u;
 #pragma unroll
           for (int kk = 0; kk < BK / 8; ++kk) {
-            const uint32_t off = kk * 32;
-            mma_tf32(dt, smem_desc(alo + off), smem_desc(bhi + off), idesc,
-                     (i == first && kk == 0) ? 0u : 1u);
-            mma_tf32(dt, smem_desc(ahi + off), smem_desc(blo + off), idesc, 1u);
-            mma_tf32(dt, smem_desc(ahi + off), smem_desc(bhi + off), idesc, 1u);
+            const uint64_t off = (uint64_t)kk * 2;  // 32 bytes per K-step
+            if (kk == 0) mma_tf32(dt, dalo + off, dbhi + off, idesc, acc0);
+            else mma_tf32_acc(dt, dalo + off, dbhi + off, idesc);
+            mma_tf32_acc(dt, dahi + off, dblo + off, idesc);
+            mma_tf32_acc(dt, dahi + off, dbhi + off, idesc);
           }
           mma_commit(empty0 + 8 * s);
           *reinterpret_cast<volatile int*>(&ctrl->commits) = i + 1;
