@@ -34,7 +34,7 @@ def test_row_tiles_match_full_tensor(spherical):
     src = IntegralSource(plan)
     for m, lay in enumerate(plan.layout):
         a = full[lay.a_offset:lay.a_offset + lay.npair * lay.naux].view(lay.npair, lay.naux)
-        tiles = src.tiles(m, max_bytes=64 * lay.naux * 8 * 8)
+        tiles = src.tiles(m, max_bytes=lay.npair * lay.naux * 8 // 5)
         assert len(tiles) > 2
         parts = [src.raw_tile(xyz, m, s0, s1) for s0, s1 in tiles]
         got = torch.cat(parts, dim=0)
