@@ -199,8 +199,12 @@ int vqc_df_gradient(const vqc_batch_desc* system, const double* xyz, const doubl
  *   vqc_ozaki_gemm: c[mol][r][n] (row stride ldc, block stride c_mol_stride)
  *     = sum_k A[mol][r][k] B[mol][n][k] from the slices of A (m rows) and B
  *     (n rows), both [mol][slice][row][ldk] (ldk % 16 == 0, k <= ldk) with
- *     their exponents, keeping slice pairs s + t <= nslices + 1.  upper != 0:
- *     B[mol][n][k] = 0 for k > n (only those K are read).  k * nslices *
+ *     their exponents, keeping slice pairs s + t <= nslices + 1.  upper = 1:
+ *     B[mol][n][k] = 0 for k > n (only those K are read); upper = 2: A and B
+ *     are the same slices (m == n) and C is symmetric: only the tiles on or
+ *     above the diagonal are formed and each element above the diagonal is
+ *     also written to its mirror (the sliced sums are exactly symmetric).
+ *     k * nslices *
  *     127^2 must stay below 2^31.  error: device int set non-zero when a
  *     bounded wait expires (the output is then invalid).
  */

@@ -117,3 +117,34 @@ def test_tensor_core_whitening_matches_fp64_whitening():
     assert rel < 1e-10, rel
     assert err.max().item() < 1e-10 * rowmax.max().item()
     chunk.close()
+
+
+@pytest.mark.parametrize("n,nmol", [(48, 3), (200, 2), (384, 1)])
+def test_symmetric_output_mode_equals_full_product(n, nmol):
+    """upper = 2 forms only the tiles on or above the diagonal of X X^T and mirrors
+    them; the sliced sums are exactly symmetric, so the result is bit-identical."""
+    rng = np.random.default_rng(n)
+    x = rng.normal(size=(nmol, n, n))
+    x = 0.5 * (x + x.transpose(0, 2, 1))
+    ns = 7
+    ldk = (n + 15) // 16 * 16
+    dx = torch.tensor(x, device="cuda")
+    sl = torch.zeros(nmol, ns, n, ldk, dtype=torch.int8, device="cuda")
+    ex = torch.empty(nmol, n, dtype=torch.int32, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    _lib.call("vqc_ozaki_slice_rows", dx.data_ptr(), nmol, n, n, n, n * n, None, ns, sl.data_ptr(),
+              ldk, ex.data_ptr(), st)
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    full = torch.full((nmol, n, n), float("nan"), dtype=torch.float64, device="cuda")
+    sym = torch.full((nmol, n, n), float("nan"), dtype=torch.float64, device="cuda")
+    for mode, out in ((0, full), (2, sym)):
+        _lib.call("vqc_ozaki_gemm", sl.data_ptr(), ex.data_ptr(), n, sl.data_ptr(), ex.data_ptr(), n,
+                  n, ldk, nmol, ns, mode, out.data_ptr(), n, n * n, err.data_ptr(), st)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    assert torch.equal(full, sym)
+    ref = np.einsum("bij,bkj->bik", x, x)
+    assert np.abs(sym.cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max()
+    with pytest.raises(_lib.VqcError):  # symmetric mode needs A == B
+        _lib.call("vqc_ozaki_gemm", sl.data_ptr(), ex.data_ptr(), n, sl.data_ptr(), err.data_ptr(), n,
+                  n, ldk, nmol, ns, 2, sym.data_ptr(), n, n * n, err.data_ptr(), st)

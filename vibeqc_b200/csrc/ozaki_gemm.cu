@@ -71,6 +71,8 @@ static_assert(SMEM <= 227 * 1024, "shared memory per CTA");
 
 struct OzParams {
   int m, n, k, ns, upper, ntn, ntm, ntiles;
+  int sym;       // symmetric output (A == B, m == n): only tiles reaching the diagonal or above
+  int sym_per;   // tiles per molecule in the symmetric layout
   const int* a_exp;  // [nmol][m]
   const int* b_exp;  // [nmol][n]
   double* c;
@@ -81,11 +83,25 @@ struct OzParams {
 // tile t -> (molecule, row tile, column tile), column tile fastest (CTAs that
 // run together share an A row block in L2)
 __device__ __forceinline__ void tile_coords(const OzParams& p, int t, int& z, int& tm, int& tn) {
+  if (p.sym) {
+    // row tile tm holds column tiles 2 tm .. ntn - 1 (BM = 2 BN): the tiles
+    // that reach the diagonal or lie above it
+    z = t / p.sym_per;
+    int r = t - z * p.sym_per;
+    tm = 0;
+    while (r >= p.ntn - 2 * tm) {
+      r -= p.ntn - 2 * tm;
+      ++tm;
+    }
+    tn = 2 * tm + r;
+    return;
+  }
   tn = t % p.ntn;
   const int r = t / p.ntn;
   tm = r % p.ntm;
   z = r / p.ntm;
 }
+static_assert(BM == 2 * BN, "the symmetric tile layout pairs one row tile with two column tiles");
 
 __device__ __forceinline__ int tile_kblocks(const OzParams& p, int tn) {
   const int kend = p.upper ? min(p.k, tn * BN + BN) : p.k;
@@ -384,6 +400,17 @@ __global__ void __launch_bounds__(kThreads, 1)
           if (n0 + c < p.n) out[c] = x2[0];
           if (n0 + c + 1 < p.n) out[c + 1] = x2[1];
         }
+        if (p.sym && row < p.m) {
+          // the mirror C[col][row] of an element above the diagonal (a warp
+          // writes 32 consecutive rows of that column); tiles below the
+          // diagonal are never computed
+          double* mir = p.c + (long long)z * p.c_mol_stride + row;
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const int col = n0 + c + e;
+            if (col < p.n && col > row) mir[(long long)col * p.ldc] = x2[e];
+          }
+        }
       }
     }
     fence_before_sync();
@@ -488,6 +515,7 @@ extern "C" int vqc_ozaki_gemm(const int8_t* a_slices, const int32_t* a_exps, int
                               int64_t ldc, int64_t c_mol_stride, int32_t* error, void* stream) {
   if (!a_slices || !a_exps || !b_slices || !b_exps || !c || m <= 0 || n <= 0 || k <= 0 ||
       ldk < k || ldk % 16 || nmol <= 0 || nslices < 1 || nslices > oz::kMaxSlices || ldc < n ||
+      upper < 0 || upper > 2 ||
       m > 0x7fffffffLL || (long long)k * nslices * 16129LL > 0x7fffffffLL ||
       (long long)nmol * nslices > 0x7fffffffLL || (m + oz::BM - 1) / oz::BM > 65535 || nmol > 65535)
     return fail(VQC_STATUS_INVALID_ARGUMENT, "ozaki_gemm: bad argument");
@@ -500,10 +528,19 @@ extern "C" int vqc_ozaki_gemm(const int8_t* a_slices, const int32_t* a_exps, int
   p.n = n;
   p.k = k;
   p.ns = nslices;
-  p.upper = upper ? 1 : 0;
+  p.upper = upper == 1 ? 1 : 0;
+  p.sym = upper == 2 ? 1 : 0;
+  if (p.sym && (m != n || a_slices != b_slices || a_exps != b_exps))
+    return fail(VQC_STATUS_INVALID_ARGUMENT, "ozaki_gemm: symmetric output needs A == B");
   p.ntn = (n + oz::BN - 1) / oz::BN;
   p.ntm = (int)((m + oz::BM - 1) / oz::BM);
-  const long long ntiles = (long long)p.ntn * p.ntm * nmol;
+  long long per = (long long)p.ntn * p.ntm;
+  if (p.sym) {
+    per = 0;
+    for (int tm = 0; tm < p.ntm; ++tm) per += std::max(0, p.ntn - 2 * tm);
+  }
+  p.sym_per = (int)per;
+  const long long ntiles = per * nmol;
   if (ntiles > 0x7fffffffLL) return fail(VQC_STATUS_INVALID_ARGUMENT, "ozaki_gemm: too many tiles");
   p.ntiles = (int)ntiles;
   p.a_exp = a_exps;

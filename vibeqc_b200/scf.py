@@ -275,8 +275,9 @@ class _SP2Graph:
         st = torch.cuda.current_stream().cuda_stream
         _lib.call("vqc_ozaki_slice_rows", x.data_ptr(), nb, n, n, n, n * n, None, SP2_SLICES,
                   self.sl.data_ptr(), self.ldk, self.ex.data_ptr(), st)
+        # symmetric output: only the tiles on or above the diagonal, mirrored
         _lib.call("vqc_ozaki_gemm", self.sl.data_ptr(), self.ex.data_ptr(), n, self.sl.data_ptr(),
-                  self.ex.data_ptr(), n, n, self.ldk, nb, SP2_SLICES, 0, self.x2.data_ptr(), n, n * n,
+                  self.ex.data_ptr(), n, n, self.ldk, nb, SP2_SLICES, 2, self.x2.data_ptr(), n, n * n,
                   self.err.data_ptr(), st)
 
     def _steps(self):
