@@ -307,6 +307,12 @@ int vqc_fitted_density_fp32_noalloc(const float* b_aux_major, const double* dens
 int vqc_anchor_combine(double* u0, const float* du_hi, const float* du_lo, float* v_hi,
                        float* v_lo, int64_t rows, int32_t x, int32_t ld_aux, double alpha,
                        int32_t mode, void* stream);
+/* vqc_coulomb_tma: the Coulomb build of vqc_coulomb_fp32 streamed by TMA
+ * (persistent CTAs, a ring of 16 KB stages, FP64 accumulation; no limit on
+ * ld_ao); error: device int set non-zero when a bounded wait expires (the
+ * output is then invalid).  Reference src/scf/cuda/df_coulomb.cpp:24. */
+int vqc_coulomb_tma(const float* b_aux_major, const double* rho, int32_t nmol, int32_t nao,
+                    int32_t ld_ao, int32_t naux, double* j, int32_t* error, void* stream);
 int vqc_coulomb_fp32(const float* b_aux_major, const double* rho, int32_t nmol, int32_t nao,
                      int32_t ld_ao, int32_t naux, double* j, void* stream);
 int vqc_fitted_density_fp32(const float* b_aux_major, const double* dens, int32_t nmol,

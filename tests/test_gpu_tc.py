@@ -161,6 +161,34 @@ def test_coulomb_fp32(nb, n, x):
     assert (j - ref).abs().max().item() <= 1e-12 * ref.abs().max().item() * x**0.5
 
 
+@pytest.mark.parametrize("nb,n,x", [(2, 40, 200), (1, 384, 1856), (3, 13, 77), (2, 520, 300)])
+def test_coulomb_tma(nb, n, x):
+    """The TMA-streamed Coulomb build against FP64 torch and the per-row kernel."""
+    ld = (n + 3) // 4 * 4
+    g = torch.Generator(device="cuda").manual_seed(5)
+    full = torch.randn(nb, n, n, x, generator=g, device="cuda", dtype=torch.float32)
+    full = 0.5 * (full + full.transpose(1, 2))
+    b = torch.zeros(nb, n, x, ld, dtype=torch.float32, device="cuda")
+    b[..., :n] = full.permute(0, 1, 3, 2)
+    del full
+    rho = torch.randn(nb, x, generator=g, device="cuda", dtype=torch.float64)
+    j = torch.full((nb, n, n), float("nan"), dtype=torch.float64, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    _lib.call("vqc_coulomb_tma", b.data_ptr(), rho.data_ptr(), nb, n, ld, x, j.data_ptr(),
+              err.data_ptr(), st)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    ref = torch.einsum("bmqn,bq->bmn", b[..., :n].double(), rho)
+    assert (j - ref).abs().max().item() <= 1e-12 * ref.abs().max().item() * x**0.5
+    assert torch.equal(j, j.transpose(1, 2))
+    if ld <= 512:
+        j2 = torch.empty_like(j)
+        _lib.call("vqc_coulomb_fp32", b.data_ptr(), rho.data_ptr(), nb, n, ld, x, j2.data_ptr(), st)
+        torch.cuda.synchronize()
+        assert (j - j2).abs().max().item() <= 1e-12 * ref.abs().max().item() * x**0.5
+
+
 @pytest.mark.parametrize("nb,n,x", [(2, 40, 200), (1, 384, 1856), (3, 13, 77)])
 def test_fitted_density_fp32(nb, n, x):
     ld = (n + 3) // 4 * 4

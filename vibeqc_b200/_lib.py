@@ -139,6 +139,8 @@ _SIGNATURES = {
                                  ctypes.c_int32, _P, _P, _P], ctypes.c_int),
     "vqc_coulomb_fp32": ([_P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                           ctypes.c_int32, _P, _P], ctypes.c_int),
+    "vqc_coulomb_tma": ([_P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                         ctypes.c_int32, _P, _P, _P], ctypes.c_int),
 }
 
 _lib = None

@@ -663,6 +663,133 @@ __global__ void __launch_bounds__(kGramThreads, 1)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Coulomb build J[mol][mu][nu] = sum_Q B[mol][mu][Q][nu] rho[mol][Q] (nu <= mu,
+// mirrored) from the FP32 aux-major tensor, streamed by TMA: persistent CTAs
+// take (mol, mu) rows largest-first in round-robin order; for each 32-column
+// nu chunk of the row the producer streams the 128-row Q blocks through a
+// ring of kCoulStages 16 KB stages, eight consumer warps (16 Q rows each, one
+// nu per lane) accumulate in FP64, and the chunk's 32 sums meet in shared
+// memory.  Reference src/scf/cuda/df_coulomb.cpp:24 (FP64 cublasDgemv).
+// ---------------------------------------------------------------------------
+
+constexpr int kCoulStages = 8;
+constexpr int kCoulWarps = 8;                       // consumers
+constexpr int kCoulThreads = 32 * (1 + kCoulWarps);  // + producer warp
+constexpr int kCoulTile = BM * BK * 4;               // 16 KB
+constexpr int kCoulSmem = kCoulStages * kCoulTile + 1024 + kCoulWarps * 32 * 8 +
+                          2 * kCoulStages * 8 + 64;
+
+struct CoulParams {
+  int nmol, nao, naux, nqt;
+  const double* rho;
+  double* j;
+  int* error;
+};
+
+__global__ void __launch_bounds__(kCoulThreads, 1)
+    coulomb_tma_kernel(const __grid_constant__ CUtensorMap tmB, CoulParams p) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  double* red = reinterpret_cast<double*>(smem + kCoulStages * kCoulTile);  // [warp][32]
+  uint64_t* bars = reinterpret_cast<uint64_t*>(red + kCoulWarps * 32);
+  __shared__ int abort_flag;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + kCoulStages);
+  if (tid == 0) {
+    for (int s = 0; s < kCoulStages; ++s) {
+      mbar_init(full0 + 8 * s, 1);
+      mbar_init(empty0 + 8 * s, kCoulWarps);
+    }
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  volatile int* ab = &abort_flag;
+  const int nitems = p.nmol * p.nao;
+  int issued = 0, consumed = 0;  // producer: tiles issued; producer copy of the consumers' count
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int g = 0;
+      bool ok = true;
+      for (int it = blockIdx.x; it < nitems && ok; it += gridDim.x) {
+        const int mu = p.nao - 1 - it / p.nmol, mol = it % p.nmol;
+        const int nkc = mu / BK + 1;
+        for (int kc = 0; kc < nkc && ok; ++kc)
+          for (int qt = 0; qt < p.nqt; ++qt, ++g) {
+            const int s = g % kCoulStages;
+            if (g >= kCoulStages && !mbar_wait(empty0 + 8 * s, ((g / kCoulStages) - 1) & 1, ab)) {
+              if (p.error) atomicExch(p.error, 51);
+              *reinterpret_cast<volatile int*>(&abort_flag) = 1;
+              ok = false;
+              break;
+            }
+            mbar_expect_tx(full0 + 8 * s, kCoulTile);
+            tma_load_3d(smem_u32(smem + s * kCoulTile), &tmB, kc * BK, qt * BM, mol * p.nao + mu,
+                        full0 + 8 * s);
+            issued = g + 1;
+          }
+      }
+      // bounded drain of copies still in flight after an abort
+      if (!ok) {
+        int never = 0;
+        for (int k = max(0, issued - kCoulStages); k < issued; ++k)
+          mbar_wait_for(full0 + 8 * (k % kCoulStages), (k / kCoulStages) & 1, &never, kWaitNs);
+      }
+    }
+  } else {  // consumers: warp w - 1 owns rows 16 (w - 1) .. + 15 of every tile, lane = nu
+    const int cw = warp - 1;
+    int g = 0;
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+      const int mu = p.nao - 1 - it / p.nmol, mol = it % p.nmol;
+      const int nkc = mu / BK + 1;
+      const double* rho = p.rho + (size_t)mol * p.naux;
+      double* jm = p.j + (size_t)mol * p.nao * p.nao;
+      for (int kc = 0; kc < nkc; ++kc) {
+        double acc = 0.0;
+        for (int qt = 0; qt < p.nqt; ++qt, ++g) {
+          const int s = g % kCoulStages;
+          // every consumer warp runs the same loops to the end, so all of them
+          // reach each named barrier below; after an abort the waits return at once
+          if (!__all_sync(0xffffffffu, mbar_wait(full0 + 8 * s, (g / kCoulStages) & 1, ab))) {
+            if (lane == 0 && p.error) atomicExch(p.error, 52);
+            *reinterpret_cast<volatile int*>(&abort_flag) = 1;
+            continue;
+          }
+          const uint8_t* tile = smem + s * kCoulTile;
+#pragma unroll
+          for (int r = 0; r < 16; ++r) {
+            const int row = cw * 16 + r;  // 128-byte swizzle: chunk (lane / 4) ^ (row % 8)
+            const int q = qt * BM + row;
+            const float b = *reinterpret_cast<const float*>(
+                tile + row * 128 + ((((lane >> 2) ^ (row & 7))) << 4) + ((lane & 3) << 2));
+            if (q < p.naux) acc = fma((double)b, __ldg(rho + q), acc);
+          }
+          __syncwarp();
+          if (lane == 0) mbar_arrive(empty0 + 8 * s);
+        }
+        red[cw * 32 + lane] = acc;
+        // the consumer warps' partial sums of this chunk (named barrier over the consumers)
+        asm volatile("bar.sync 1, %0;" ::"r"(32 * kCoulWarps) : "memory");
+        if (cw == 0) {
+          double v = 0.0;
+#pragma unroll
+          for (int w = 0; w < kCoulWarps; ++w) v += red[w * 32 + lane];
+          const int nu = kc * BK + lane;
+          if (nu <= mu && !*ab) {
+            jm[(size_t)mu * p.nao + nu] = v;
+            jm[(size_t)nu * p.nao + mu] = v;
+          }
+        }
+        asm volatile("bar.sync 1, %0;" ::"r"(32 * kCoulWarps) : "memory");
+      }
+    }
+  }
+  (void)consumed;
+}
+
 // Self-test of the bounded-wait error path: one warp waits on an mbarrier
 // that nothing ever arrives on; the wait must give up after budget_ns and
 // the kernel must report it in *error and return normally.
@@ -858,4 +985,31 @@ extern "C" int vqc_tc_gram_sym2(const float* a_hi, const float* a_lo, const floa
   if (!a_hi || !a_lo || !b_hi || !b_lo || !kout || nmol <= 0 || nao <= 0 || kdim <= 0 || kdim % 4)
     return fail(VQC_STATUS_INVALID_ARGUMENT, "gram_sym2: bad argument");
   return launch_gram(a_hi, a_lo, b_hi, b_lo, 2, nmol, nao, kdim, kout, error, stream);
+}
+
+extern "C" int vqc_coulomb_tma(const float* b_aux_major, const double* rho, int32_t nmol,
+                               int32_t nao, int32_t ld_ao, int32_t naux, double* j, int32_t* error,
+                               void* stream) {
+  if (!b_aux_major || !rho || !j || !error || nmol <= 0 || nao <= 0 || naux <= 0 || ld_ao < nao ||
+      ld_ao % 4 || (long long)nmol * nao > 0x7fffffffLL)
+    return fail(VQC_STATUS_INVALID_ARGUMENT, "coulomb_tma: bad argument");
+  CUtensorMap tb;
+  int st = make_map(&tb, b_aux_major, nao, ld_ao, naux, nmol * nao, BM);
+  if (st) return st;
+  CoulParams p{};
+  p.nmol = nmol;
+  p.nao = nao;
+  p.naux = naux;
+  p.nqt = (naux + BM - 1) / BM;
+  p.rho = rho;
+  p.j = j;
+  p.error = error;
+  cudaError_t e = cudaFuncSetAttribute(coulomb_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       kCoulSmem);
+  if (e != cudaSuccess) return cuda_status(e, "coulomb_tma smem attribute");
+  const int items = nmol * nao;
+  const int ctas = items < sm_count() ? items : sm_count();
+  coulomb_tma_kernel<<<ctas, kCoulThreads, kCoulSmem, (cudaStream_t)stream>>>(tb, p);
+  count_launch();
+  return cuda_status(cudaGetLastError(), "coulomb_tma");
 }

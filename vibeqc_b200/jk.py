@@ -175,8 +175,8 @@ class MixedBuilder:
             self._half(c_occ, dens=dd, rho_dens=self.rho)
             j = torch.empty(nb, n, n, dtype=torch.float64, device=d.device)
             with TIMER.stage("J_fp32"):
-                self._lib.call("vqc_coulomb_fp32", self.b.data_ptr(), self.rho.data_ptr(), nb, n,
-                               self.ld, self.x, j.data_ptr(), self.st)
+                self._lib.call("vqc_coulomb_tma", self.b.data_ptr(), self.rho.data_ptr(), nb, n,
+                               self.ld, self.x, j.data_ptr(), self.err.data_ptr(), self.st)
         else:
             self._half(c_occ)
         k = torch.zeros(nb, n, n, dtype=torch.float64, device=d.device)
@@ -250,8 +250,8 @@ class MixedBuilder:
         if with_j:
             dj = torch.empty(nb, n, n, dtype=torch.float64, device=d.device)
             with TIMER.stage("J_fp32"):
-                self._lib.call("vqc_coulomb_fp32", self.b.data_ptr(), drho.data_ptr(), nb, n,
-                               self.ld, x, dj.data_ptr(), self.st)
+                self._lib.call("vqc_coulomb_tma", self.b.data_ptr(), drho.data_ptr(), nb, n,
+                               self.ld, x, dj.data_ptr(), self.err.data_ptr(), self.st)
             j = anc["j0"] + dj
         COUNTERS["k_flops"] += 2 * nb * x * o * n * (n + 1)  # V dU^T + dU V^T
         with TIMER.stage("K_gram_tc"):

@@ -171,8 +171,8 @@ def _coulomb_fp32(jk, drho: torch.Tensor) -> torch.Tensor:
     nb, n = jk.nb, jk.n
     out = torch.empty(nb, n, n, dtype=torch.float64, device=drho.device)
     with TIMER.stage("J_fp32"):
-        jk._lib.call("vqc_coulomb_fp32", jk.b.data_ptr(), drho.contiguous().data_ptr(), nb, n,
-                     jk.ld, jk.x, out.data_ptr(), jk.st)
+        jk._lib.call("vqc_coulomb_tma", jk.b.data_ptr(), drho.contiguous().data_ptr(), nb, n,
+                     jk.ld, jk.x, out.data_ptr(), jk.err.data_ptr(), jk.st)
     return out
 
 
