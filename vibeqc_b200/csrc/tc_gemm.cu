@@ -677,8 +677,9 @@ constexpr int kCoulStages = 8;
 constexpr int kCoulWarps = 8;                       // consumers
 constexpr int kCoulThreads = 32 * (1 + kCoulWarps);  // + producer warp
 constexpr int kCoulTile = BM * BK * 4;               // 16 KB
+constexpr int kCoulMaxAux = 4096;  // fitted-density entries staged in shared memory
 constexpr int kCoulSmem = kCoulStages * kCoulTile + 1024 + kCoulWarps * 32 * 8 +
-                          2 * kCoulStages * 8 + 64;
+                          2 * kCoulStages * 8 + kCoulMaxAux * 8 + 64;
 
 struct CoulParams {
   int nmol, nao, naux, nqt;
@@ -694,6 +695,7 @@ __global__ void __launch_bounds__(kCoulThreads, 1)
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
   double* red = reinterpret_cast<double*>(smem + kCoulStages * kCoulTile);  // [warp][32]
   uint64_t* bars = reinterpret_cast<uint64_t*>(red + kCoulWarps * 32);
+  double* srho = reinterpret_cast<double*>(bars + 2 * kCoulStages);  // [nqt * BM]
   __shared__ int abort_flag;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + kCoulStages);
@@ -742,13 +744,21 @@ __global__ void __launch_bounds__(kCoulThreads, 1)
   } else {  // consumers: warp w - 1 owns rows 16 (w - 1) .. + 15 of every tile, lane = nu
     const int cw = warp - 1;
     int g = 0;
+    int rho_mol = -1;
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
       const int mu = p.nao - 1 - it / p.nmol, mol = it % p.nmol;
       const int nkc = mu / BK + 1;
-      const double* rho = p.rho + (size_t)mol * p.naux;
       double* jm = p.j + (size_t)mol * p.nao * p.nao;
+      if (mol != rho_mol) {
+        // the molecule's fitted density in shared memory (zero beyond naux)
+        asm volatile("bar.sync 1, %0;" ::"r"(32 * kCoulWarps) : "memory");
+        for (int q = tid - 32; q < p.nqt * BM; q += 32 * kCoulWarps)
+          srho[q] = q < p.naux ? __ldg(p.rho + (size_t)mol * p.naux + q) : 0.0;
+        asm volatile("bar.sync 1, %0;" ::"r"(32 * kCoulWarps) : "memory");
+        rho_mol = mol;
+      }
       for (int kc = 0; kc < nkc; ++kc) {
-        double acc = 0.0;
+        double acc4[4] = {0.0, 0.0, 0.0, 0.0};  // independent chains over the rows
         for (int qt = 0; qt < p.nqt; ++qt, ++g) {
           const int s = g % kCoulStages;
           // every consumer warp runs the same loops to the end, so all of them
@@ -759,18 +769,18 @@ __global__ void __launch_bounds__(kCoulThreads, 1)
             continue;
           }
           const uint8_t* tile = smem + s * kCoulTile;
+          const double* rq = srho + qt * BM + cw * 16;
 #pragma unroll
           for (int r = 0; r < 16; ++r) {
             const int row = cw * 16 + r;  // 128-byte swizzle: chunk (lane / 4) ^ (row % 8)
-            const int q = qt * BM + row;
             const float b = *reinterpret_cast<const float*>(
                 tile + row * 128 + ((((lane >> 2) ^ (row & 7))) << 4) + ((lane & 3) << 2));
-            if (q < p.naux) acc = fma((double)b, __ldg(rho + q), acc);
+            acc4[r & 3] = fma((double)b, rq[r], acc4[r & 3]);  // rows >= naux read as zero
           }
           __syncwarp();
           if (lane == 0) mbar_arrive(empty0 + 8 * s);
         }
-        red[cw * 32 + lane] = acc;
+        red[cw * 32 + lane] = (acc4[0] + acc4[1]) + (acc4[2] + acc4[3]);
         // the consumer warps' partial sums of this chunk (named barrier over the consumers)
         asm volatile("bar.sync 1, %0;" ::"r"(32 * kCoulWarps) : "memory");
         if (cw == 0) {
@@ -991,7 +1001,8 @@ extern "C" int vqc_coulomb_tma(const float* b_aux_major, const double* rho, int3
                                int32_t nao, int32_t ld_ao, int32_t naux, double* j, int32_t* error,
                                void* stream) {
   if (!b_aux_major || !rho || !j || !error || nmol <= 0 || nao <= 0 || naux <= 0 || ld_ao < nao ||
-      ld_ao % 4 || (long long)nmol * nao > 0x7fffffffLL)
+      ld_ao % 4 || (long long)nmol * nao > 0x7fffffffLL ||
+      (naux + BM - 1) / BM * BM > kCoulMaxAux)
     return fail(VQC_STATUS_INVALID_ARGUMENT, "coulomb_tma: bad argument");
   CUtensorMap tb;
   int st = make_map(&tb, b_aux_major, nao, ld_ao, naux, nmol * nao, BM);
