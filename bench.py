@@ -306,6 +306,11 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
               "peak_source": peaks["source"],
               "traffic_note": "dram read+write per launch scaled from an ncu capture of (H2O)12 x 8 "
                               f"(measured/algorithmic = {HALF_TRAFFIC_RATIO})"}
+        if kc.get("half_min_bytes"):
+            # the kernel streams full N x N rows of B and writes U split (hi, lo);
+            # a symmetric-packed form would move only this floor
+            rl["frac_vs_packed_floor"] = round(kc["half_min_bytes"] / t_half / 1e9 / peaks["hbm_gbs"], 4)
+            rl["packed_floor_bytes_per_launch"] = round(kc["half_min_bytes"] / kc["half_launches"])
     out = {
         "metric": METRIC,
         "value": round(value, 3),

@@ -154,7 +154,11 @@ struct HalfCfg {
   static constexpr int STAGE = 2 * A_BYTES + 2 * C_BYTES;
   static constexpr int S = (214 * 1024) / STAGE >= 4 ? 4 : (214 * 1024) / STAGE;
   static constexpr int SMEM = S * STAGE + 1024 + (int)sizeof(Ctrl) + 64;
-  static_assert(BN % 16 == 0 && BN >= 16 && BN <= kTmemBuf, "BN");
+  // TMEM columns per accumulator buffer: [0, BN) takes A_hi C_hi + A_lo C_hi,
+  // [BN, 2 BN) takes A_hi C_lo (one N = 2 BN MMA over the adjacent C_hi, C_lo
+  // tiles); allocations are powers of two
+  static constexpr int TBUF = 2 * BN <= 128 ? 128 : 256;
+  static_assert(BN % 16 == 0 && BN >= 16 && 2 * BN <= 256, "BN");
   static_assert(S >= 2, "pipeline");
 };
 
@@ -200,7 +204,7 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(&ctrl->tmem)),
-                 "r"(2 * kTmemBuf)
+                 "r"(2 * C::TBUF)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -331,7 +335,7 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
   split_done:;
   } else if (warp == kMmaWarp) {
     if (lane == 0) {  // MMA issuer
-      constexpr uint32_t idesc = instr_desc<BN>();
+      constexpr uint32_t idesc = instr_desc<BN>(), idesc2 = instr_desc<2 * BN>();
       int g = 0, t = 0;
       const int i0 = blockIdx.x * p.per_cta, i1 = min(p.nitems, i0 + p.per_cta);
       for (int item = i0; item < i1 && !aborted(ctrl); ++item, ++t) {
@@ -341,7 +345,7 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
           break;
         }
         fence_after_sync();
-        const uint32_t dt = tmem + b * kTmemBuf;
+        const uint32_t dt = tmem + b * C::TBUF;
         bool ok = true;
         for (int kb = 0; kb < nk; ++kb, ++g) {
           const int s = g % S;
@@ -354,16 +358,16 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
           // descriptors advance by (byte offset >> 4) in their address field
           const uint32_t ahi = smem_u32(stage(s));
           const uint64_t dahi = smem_desc(ahi), dalo = smem_desc(ahi + C::A_BYTES);
+          // C_lo directly follows C_hi (C_BYTES = BN rows of 128 bytes), so one
+          // descriptor spans both as a 2 BN-row operand
           const uint64_t dchi = smem_desc(ahi + 2 * C::A_BYTES);
-          const uint64_t dclo = smem_desc(ahi + 2 * C::A_BYTES + C::C_BYTES);
           const uint32_t acc0 = kb == 0 ? 0u : 1u;
 #pragma unroll
           for (int kk = 0; kk < BK / 8; ++kk) {
             const uint64_t off = (uint64_t)kk * 2;  // 32 bytes per K-step
-            if (kk == 0) mma_tf32(dt, dalo + off, dchi + off, idesc, acc0);
-            else mma_tf32_acc(dt, dalo + off, dchi + off, idesc);
-            mma_tf32_acc(dt, dahi + off, dclo + off, idesc);
-            mma_tf32_acc(dt, dahi + off, dchi + off, idesc);
+            if (kk == 0) mma_tf32(dt, dahi + off, dchi + off, idesc2, acc0);
+            else mma_tf32_acc(dt, dahi + off, dchi + off, idesc2);
+            mma_tf32_acc(dt, dalo + off, dchi + off, idesc);
           }
           mma_commit(empty0 + 8 * s);
           *reinterpret_cast<volatile int*>(&ctrl->commits) = g + 1;
@@ -406,8 +410,12 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
       const double* cv = p.cvec + (size_t)z * p.nocc;
 #pragma unroll
       for (int c = 16 * half; c < BN; c += 16 * kEpiGroups) {
-        float v[16];
-        tmem_ld16(tmem + b * kTmemBuf + ((uint32_t)(q * 32) << 16) + c, v);
+        float v[16], w[16];
+        const uint32_t tb = tmem + b * C::TBUF + ((uint32_t)(q * 32) << 16) + c;
+        tmem_ld16(tb, v);
+        tmem_ld16(tb + BN, w);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) v[k] += w[k];
         if (valid) {
 #pragma unroll
           for (int k = 0; k < 16; ++k) {
@@ -449,7 +457,7 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
   if (warp == 0) {
     fence_after_sync();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                 "r"(2 * kTmemBuf)
+                 "r"(2 * C::TBUF)
                  : "memory");
   }
 }
@@ -505,6 +513,9 @@ __global__ void __launch_bounds__(kGramThreads, 1)
   const int nkb = kb1 - kb0;
   if (nkb <= 0 || mt >= p.nt) return;
   const int nchains = (nkb + kGramFlush - 1) / kGramFlush;
+  // MMA width: the tile's in-range columns rounded up to 16 (M = 128 allows
+  // N = 16..256 in steps of 16); TMEM columns past it are never read
+  const int nmma = min(BN, (p.nao - nt * BN + 15) & ~15);
 
   const uint32_t full0 = smem_u32(ctrl->full), empty0 = smem_u32(ctrl->empty);
   const uint32_t af0 = smem_u32(ctrl->acc_full), ae0 = smem_u32(ctrl->acc_empty);
@@ -565,7 +576,7 @@ __global__ void __launch_bounds__(kGramThreads, 1)
     }
   } else if (warp == 1) {
     if (lane == 0) {  // MMA issuer
-      constexpr uint32_t idesc = instr_desc<BN>();
+      const uint32_t idesc = (instr_desc<BN>() & ~(0x3fu << 17)) | ((uint32_t)(nmma >> 3) << 17);
       int i = 0;
       for (int ch = 0; ch < nchains && !aborted(ctrl); ++ch) {
         const int b = ch & 1;
@@ -617,6 +628,7 @@ __global__ void __launch_bounds__(kGramThreads, 1)
       fence_after_sync();
 #pragma unroll
       for (int c = 0; c < 64; c += 16) {
+        if (half * 64 + c >= nmma) continue;  // warp-uniform
         float v[16];
         tmem_ld16(tmem + b * kTmemBuf + half * 64 + c + ((uint32_t)(q * 32) << 16), v);
 #pragma unroll

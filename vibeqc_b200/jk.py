@@ -25,8 +25,10 @@ from .timing import TIMER
 # algorithmic work of the tensor-core exchange since the last reset (host-side
 # tallies, read by the benchmark): bytes the half transform must move (FP32 B
 # read once, split U written), its launches, and the exchange flops counted
-# once (half transform 2 N^2 X o, Gram X o N (N + 1) per term)
-COUNTERS = {"half_bytes": 0, "half_launches": 0, "k_flops": 0}
+# once (half transform 2 N^2 X o, Gram X o N (N + 1) per term); "half_min_bytes"
+# is the floor of a symmetric-packed kernel: the mu >= nu half of the FP32 B
+# read once and U written once in FP32
+COUNTERS = {"half_bytes": 0, "half_min_bytes": 0, "half_launches": 0, "k_flops": 0}
 
 
 def reset_counters() -> None:
@@ -152,6 +154,7 @@ class MixedBuilder:
                        ct.numel(), self.st)
         c64 = (c_occ if cvec is None else cvec).contiguous()
         COUNTERS["half_bytes"] += nb * n * self.x * self.ld * 4 + nb * n * o * self.ldq * 8
+        COUNTERS["half_min_bytes"] += nb * (n * (n + 1) // 2 * self.x * 4 + n * o * self.x * 4)
         COUNTERS["half_launches"] += 1
         COUNTERS["k_flops"] += 2 * nb * n * n * self.x * o
         with TIMER.stage("K_half_tc"):
