@@ -243,9 +243,10 @@ int vqc_sp2_update(const double* x, const double* x2, double* xout, int32_t nmol
  *     [mol][nao][nocc] FP64; o_pad = MMA N (round_up(nocc,16) <= 128).
  *     With dens (D [mol][nao][nao] FP64, NULL to skip) the same pass also
  *     adds the fitted density rho_dens[mol][Q] += sum_{mu,nu} B[mu][Q][nu]
- *     D[mu][nu] (FP64 products of the exact FP32 B values; dens and rho_dens
- *     both set or both NULL), so a build needs no separate fitted-density
- *     pass over B.
+ *     D[mu][nu] (four-term FP32 partial sums of the exact FP32 B values
+ *     times D rounded to FP32, accumulated in FP64: error within a few 2^-24
+ *     of sum |B| |D|; dens and rho_dens both set or both NULL), so a build
+ *     needs no separate fitted-density pass over B.
  *     Reference src/scf/cuda/df_occupied_exchange.cpp:251-257 (U = B C) and
  *     src/scf/cuda/df_coulomb.cpp:38-57 (rho = B^T vec(D)).
  *   vqc_tc_gram: kout[mol] += U U^T over kdim = nocc * ld_aux from the split

@@ -5,15 +5,19 @@
 //     A B^T = A_hi B_hi^T + A_hi B_lo^T + A_lo B_hi^T,
 // x_hi = rn_tf32(x), x_lo = rn_tf32(x - x_hi): round-to-nearest splitting, so
 // the products carry ~2^-22 relative error without the one-sided bias of
-// truncation.  Operand tiles arrive by TMA (128-byte swizzle, K-major).
+// truncation.  The streamed B tile of the half transform is the exception:
+// the MMA reads its FP32 values, whose TF32 truncation is x_hi, and
+// x_lo = rn_tf32(x - x_hi) (exact residual, rounded to nearest) carries the
+// rest, so the split stays unbiased (~2^-22 per element) without writing x_hi
+// back.  Operand tiles arrive by TMA (128-byte swizzle, K-major).
 //
 //   half_ws_kernel -- U[mol][mu][Q][i] = sum_nu B[mol][mu][Q][nu] C[nu][i]
 //     (reference src/scf/cuda/df_occupied_exchange.cpp:251-257).  Persistent
 //     over (mu, 128-row Q tile) items; each CTA takes a contiguous item range
 //     with mu fastest, so rho rows accumulate in registers across items.  U is
 //     written as [mol][mu][i][Q] (Q contiguous: coalesced epilogue stores).
-//     Warp roles: one TMA producer, eight splitter warps that split the
-//     streamed FP32 B tile (hi in place, lo in a sibling buffer), one
+//     Warp roles: one TMA producer, eight splitter warps that write the
+//     streamed FP32 B tile's lo part into a sibling buffer, one
 //     MMA-issuing thread, eight epilogue warps (two per TMEM lane quarter).
 //     C arrives pre-split.  Two TMEM accumulators let an item's epilogue (U
 //     written already split, rho[Q] += 2 sum_i U C[mu][i] for J) overlap the next
@@ -93,12 +97,10 @@ __device__ __forceinline__ float rn_tf32(float x) {
   return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
 }
 
-__device__ __forceinline__ void split4(float4& v, float4& lo) {
-  float h;
-  h = rn_tf32(v.x); lo.x = rn_tf32(v.x - h); v.x = h;
-  h = rn_tf32(v.y); lo.y = rn_tf32(v.y - h); v.y = h;
-  h = rn_tf32(v.z); lo.z = rn_tf32(v.z - h); v.z = h;
-  h = rn_tf32(v.w); lo.w = rn_tf32(v.w - h); v.w = h;
+// x with its 13 low mantissa bits cleared: the TF32 value the tensor core
+// takes from an FP32 operand; x - tf32_trunc(x) is exact in FP32
+__device__ __forceinline__ float tf32_trunc(float x) {
+  return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u);
 }
 
 
@@ -124,7 +126,8 @@ __device__ __forceinline__ bool aborted(Ctrl* c) {
 // ---------------------------------------------------------------------------
 // half transform: U[z][Q][i] = sum_nu B[z][Q][nu] C[mol(z)][i][nu], 3xTF32,
 // persistent over (z, 128-row Q tile) items; warp roles:
-//   w0 TMA producer, w1-w8 splitters (A -> hi in place + lo), w9 MMA issuer,
+//   w0 TMA producer, w1-w8 splitters (A -> lo; the MMA reads A_hi as the TF32
+//   truncation of the FP32 tile), w9 MMA issuer,
 //   w10-w17 epilogue (TMEM -> U hi/lo in HBM, rho partial sums)
 // ---------------------------------------------------------------------------
 
@@ -243,8 +246,10 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
     int g = 0;
     const int i0 = blockIdx.x * p.per_cta, i1 = min(p.nitems, i0 + p.per_cta);
     // With p.dens the splitters also form the fitted density from the exact
-    // FP32 values they split: rho_dens[Q] += sum_nu B[mu][Q][nu] D[mu][nu] in
-    // FP64.  Float4 k of a 128-byte-swizzled stage holds row r = k / 8 and
+    // FP32 values they split: rho_dens[Q] += sum_nu B[mu][Q][nu] D[mu][nu],
+    // four-term FP32 partial sums accumulated in FP64 (relative error ~2^-23
+    // of sum |B D|; only the tensor-core phase before the FP64 anchor uses
+    // it).  Float4 k of a 128-byte-swizzled stage holds row r = k / 8 and
     // logical chunk (k % 8) ^ (r % 8); this thread's rows are ts / 8 + 32 i
     // (i < 4), all in the same chunk, so its four nu are fixed per K-block and
     // the eight lanes sharing a row cover its 32 columns.
@@ -290,9 +295,10 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
       (void)mu;
       for (int kb = 0; kb < nk; ++kb, ++g) {
         const int s = g % S;
-        // this K-block's density weights were loaded one step ahead; fetch
-        // the next step's now, before the barrier wait hides their latency
-        const double w0 = wn[0], w1 = wn[1], w2 = wn[2], w3 = wn[3];
+        // this K-block's density weights were loaded one step ahead (kept in
+        // FP64 until here so no conversion waits on the load); fetch the next
+        // step's now, before the barrier wait hides their latency
+        const float w0 = (float)wn[0], w1 = (float)wn[1], w2 = (float)wn[2], w3 = (float)wn[3];
         if (kb + 1 < nk) load_weights(item, kb + 1, wn);
         else load_weights(item + 1, 0, wn);
         // every lane waits; the warp leaves together (no lane may skip a
@@ -302,17 +308,21 @@ __global__ void __launch_bounds__(kHalfThreads, 1)
           goto split_done;
         }
         if (ts == 0) *reinterpret_cast<volatile int*>(&ctrl->consumed) = g + 1;
-        float4* a = reinterpret_cast<float4*>(stage(s));
+        // the FP32 tile stays in place: the MMA takes its TF32 truncation as
+        // A_hi, and the splitters write A_lo = rn_tf32(x - tf32_trunc(x))
+        const float4* a = reinterpret_cast<const float4*>(stage(s));
         float4* alo = reinterpret_cast<float4*>(stage(s) + C::A_BYTES);
 #pragma unroll
         for (int i = 0; i < kRowsPerThread; ++i) {
           const int k = ts + i * 32 * kSplitWarps;
-          float4 v = a[k], lo;
+          const float4 v = a[k];
           if (p.dens)
-            racc[i] = fma((double)v.x, w0, fma((double)v.y, w1,
-                      fma((double)v.z, w2, fma((double)v.w, w3, racc[i]))));
-          split4(v, lo);
-          a[k] = v;
+            racc[i] += (double)fmaf(v.x, w0, fmaf(v.y, w1, fmaf(v.z, w2, v.w * w3)));
+          float4 lo;
+          lo.x = rn_tf32(v.x - tf32_trunc(v.x));
+          lo.y = rn_tf32(v.y - tf32_trunc(v.y));
+          lo.z = rn_tf32(v.z - tf32_trunc(v.z));
+          lo.w = rn_tf32(v.w - tf32_trunc(v.w));
           alo[k] = lo;
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");

@@ -171,8 +171,9 @@ class MixedBuilder:
         j = None
         if with_j:
             # the fitted density rho = B^T vec(D) comes from the half
-            # transform's own pass over the FP32 B (FP64 products of the exact
-            # FP32 values, no tensor-core accumulation error in J), then J = B rho
+            # transform's own pass over the FP32 B (FP32 partial sums of the
+            # exact FP32 values accumulated in FP64, no tensor-core
+            # accumulation error in J), then J = B rho
             dd = d.contiguous()
             self.rho.zero_()
             self._half(c_occ, dens=dd, rho_dens=self.rho)
