@@ -526,6 +526,9 @@ __global__ void __launch_bounds__(kGramThreads, 1)
   // MMA width: the tile's in-range columns rounded up to 16 (M = 128 allows
   // N = 16..256 in steps of 16); TMEM columns past it are never read
   const int nmma = min(BN, (p.nao - nt * BN + 15) & ~15);
+  // a diagonal tile of A A^T multiplies a row block by itself: one copy of
+  // the operands serves both sides
+  const bool diag = p.nseg == 1 && mt == nt;
 
   const uint32_t full0 = smem_u32(ctrl->full), empty0 = smem_u32(ctrl->empty);
   const uint32_t af0 = smem_u32(ctrl->acc_full), ae0 = smem_u32(ctrl->acc_empty);
@@ -576,11 +579,13 @@ __global__ void __launch_bounds__(kGramThreads, 1)
         const CUtensorMap* rl = seg ? &tmBL : &tmAL;
         const CUtensorMap* ch = (one || seg) ? &tmAH : &tmBH;
         const CUtensorMap* cl = (one || seg) ? &tmAL : &tmBL;
-        mbar_expect_tx(full0 + 8 * s, C::STAGE);
+        mbar_expect_tx(full0 + 8 * s, diag ? 2 * C::TILE : C::STAGE);
         tma_load_3d(a, rh, k, mt * BM, z, full0 + 8 * s);
         tma_load_3d(a + C::TILE, rl, k, mt * BM, z, full0 + 8 * s);
-        tma_load_3d(a + 2 * C::TILE, ch, k, nt * BN, z, full0 + 8 * s);
-        tma_load_3d(a + 3 * C::TILE, cl, k, nt * BN, z, full0 + 8 * s);
+        if (!diag) {
+          tma_load_3d(a + 2 * C::TILE, ch, k, nt * BN, z, full0 + 8 * s);
+          tma_load_3d(a + 3 * C::TILE, cl, k, nt * BN, z, full0 + 8 * s);
+        }
         *reinterpret_cast<volatile int*>(&ctrl->issued) = i + 1;
       }
     }
@@ -610,7 +615,8 @@ __global__ void __launch_bounds__(kGramThreads, 1)
           // descriptors advance by (byte offset >> 4) in their address field
           const uint32_t ahi = smem_u32(stage(s));
           const uint64_t dahi = smem_desc(ahi), dalo = smem_desc(ahi + C::TILE);
-          const uint64_t dbhi = smem_desc(ahi + 2 * C::TILE), dblo = smem_desc(ahi + 3 * C::TILE);
+          const uint64_t dbhi = diag ? dahi : smem_desc(ahi + 2 * C::TILE);
+          const uint64_t dblo = diag ? dalo : smem_desc(ahi + 3 * C::TILE);
           const uint32_t acc0 = i == first ? 0u : 1u;
 #pragma unroll
           for (int kk = 0; kk < BK / 8; ++kk) {
