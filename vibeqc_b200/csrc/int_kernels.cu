@@ -113,6 +113,7 @@ __global__ void __launch_bounds__(Int3cCfg<LA, LB, LC, SPH>::THREADS, min_ctas3c
         const double b = orb.exps[pb0 + ib], cb_ = orb.coefs[pb0 + ib];
         const double p = a + b, ip = 1.0 / p;
         const double kab = exp(-a * b * ip * rab2) * ca_ * cb_;
+        if (fabs(kab) < kPrimPairCut) continue;
         const double P[3] = {(a * A[0] + b * B[0]) * ip, (a * A[1] + b * B[1]) * ip,
                              (a * A[2] + b * B[2]) * ip};
         for (int ic = 0; ic < nc; ++ic) {
@@ -249,6 +250,7 @@ __global__ void __launch_bounds__(rp_threads3c(LA, LB, LC, SPH))
         const double b = orb.exps[pb0 + ib], cb_ = orb.coefs[pb0 + ib];
         const double p = a + b, ip = 1.0 / p;
         const double kab = exp(-a * b * ip * rab2) * ca_ * cb_;
+        if (fabs(kab) < kPrimPairCut) continue;
         const double P[3] = {(a * A[0] + b * B[0]) * ip, (a * A[1] + b * B[1]) * ip,
                              (a * A[2] + b * B[2]) * ip};
         for (int ic = 0; ic < nc; ++ic) {
