@@ -247,7 +247,8 @@ __host__ __device__ constexpr int rp_threads_g3c(int la, int lb, int lc, bool sp
 }
 
 template <int LA, int LB, int LC, bool SPH>
-__global__ void __launch_bounds__(rp_threads_g3c(LA, LB, LC, SPH))
+__global__ void __launch_bounds__(rp_threads_g3c(LA, LB, LC, SPH),
+                                  min_ctas_rp(rp_threads_g3c(LA, LB, LC, SPH)))
     grad3c_rp_kernel(DevBasis orb, DevBasis aux, const double* __restrict__ xyz,
                      const DevMol* __restrict__ mols, const int2* __restrict__ pairs,
                      const ClassMol* __restrict__ cms, int ncm, const double* __restrict__ abar,

@@ -204,7 +204,7 @@ __host__ __device__ constexpr int rp_threads3c(int la, int lb, int lc, bool sph)
 }
 
 template <int LA, int LB, int LC, bool SPH>
-__global__ void __launch_bounds__(rp_threads3c(LA, LB, LC, SPH))
+__global__ void __launch_bounds__(rp_threads3c(LA, LB, LC, SPH), min_ctas_rp(rp_threads3c(LA, LB, LC, SPH)))
     int3c_rp_kernel(DevBasis orb, DevBasis aux, const double* __restrict__ xyz,
                     const DevMol* __restrict__ mols, const int2* __restrict__ pairs,
                     const ClassMol* __restrict__ cms, int ncm, double* __restrict__ out) {

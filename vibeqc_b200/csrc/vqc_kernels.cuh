@@ -59,6 +59,11 @@ __host__ __device__ constexpr int min_ctas3c(int la, int lb, int lc) {
 __host__ __device__ constexpr int min_ctas_grad3c(int la, int lb, int lc) {
   return la + lb + lc <= 5 ? 2 : 1;
 }
+// Resident CTAs per SM requested for the root-parallel 3-centre kernels:
+// enough for about 512 threads per SM (at most 128 registers a thread).
+__host__ __device__ constexpr int min_ctas_rp(int threads) {
+  return threads >= 512 ? 1 : (512 / threads > 8 ? 8 : 512 / threads);
+}
 
 template <int LA, int LB, int LC, bool SPH>
 struct Int3cCfg {
