@@ -268,46 +268,61 @@ __global__ void __launch_bounds__(rp_threads_g3c(LA, LB, LC, SPH),
   const int slot = threadIdx.x / NR, r = threadIdx.x % NR;
   const int t = t0 + slot;
   const bool valid = slot < C::SLOTS && t < cm.ntriples;
+  // contraction weights of every Cartesian aux component, Cartesian in a and
+  // b: one copy per slot in shared memory, formed by the slot's first root
+  // thread and read by all of its roots (a register copy per root thread held
+  // these kernels at 126-255 registers)
+  __shared__ double wsh[C::SLOTS][NCC * NCA * NCB];
   double gA[3] = {0.0, 0.0, 0.0}, gB[3] = {0.0, 0.0, 0.0};
   int atomA = -1, atomB = -1, atomC = -1;
+  int2 pr = make_int2(0, 0);
+  int sc = 0;
+  bool work = false;
   if (valid) {
-    const int2 pr = pairs[cm.pair_begin + t / cm.naux];
-    const int sc = cm.aux_begin + t % cm.naux;
+    pr = pairs[cm.pair_begin + t / cm.naux];
+    sc = cm.aux_begin + t % cm.naux;
     atomA = orb.atom[pr.x];
     atomB = orb.atom[pr.y];
     atomC = aux.atom[sc];
-    if (!(atomA == atomB && atomB == atomC)) {
-      const DevMol mol = mols[cm.mol];
-      // weights of every Cartesian aux component, Cartesian in a and b
-      double wc[NCC][NCA][NCB];
-      const int fa = orb.func_off[pr.x], fb = orb.func_off[pr.y], fc = aux.func_off[sc];
-      {
-        double wk[NOA][NOB][NOC];
+    work = !(atomA == atomB && atomB == atomC);
+  }
+  if (work && r == 0) {
+    const DevMol mol = mols[cm.mol];
+    const int fa = orb.func_off[pr.x], fb = orb.func_off[pr.y], fc = aux.func_off[sc];
+    double wk[NOA][NOB][NOC];
 #pragma unroll
-        for (int i = 0; i < NOA; ++i)
+    for (int i = 0; i < NOA; ++i)
 #pragma unroll
-          for (int j = 0; j < NOB; ++j) {
-            const long long mu = fa + i, nu = fb + j;
-            const long long hi = mu > nu ? mu : nu, lo = mu > nu ? nu : mu;
-            const double* row = abar + mol.a_off + (hi * (hi + 1) / 2 + lo) * mol.naux + fc;
+      for (int j = 0; j < NOB; ++j) {
+        const long long mu = fa + i, nu = fb + j;
+        const long long hi = mu > nu ? mu : nu, lo = mu > nu ? nu : mu;
+        const double* row = abar + mol.a_off + (hi * (hi + 1) / 2 + lo) * mol.naux + fc;
 #pragma unroll
-            for (int k = 0; k < NOC; ++k) wk[i][j][k] = __ldg(row + k);
-          }
-#pragma unroll
-        for (int z = 0; z < NCC; ++z) {
-          double wsph[NOA][NOB];
-#pragma unroll
-          for (int i = 0; i < NOA; ++i)
-#pragma unroll
-            for (int j = 0; j < NOB; ++j) {
-              double s = 0.0;
-#pragma unroll
-              for (int k = 0; k < NOC; ++k) s = fma(c_trans[MODE][LC][k][z], wk[i][j][k], s);
-              wsph[i][j] = s;
-            }
-          weights_to_cart<LA, LB, NOA, NOB>(MODE, wsph, wc[z]);
-        }
+        for (int k = 0; k < NOC; ++k) wk[i][j][k] = __ldg(row + k);
       }
+#pragma unroll
+    for (int z = 0; z < NCC; ++z) {
+      double wsph[NOA][NOB];
+#pragma unroll
+      for (int i = 0; i < NOA; ++i)
+#pragma unroll
+        for (int j = 0; j < NOB; ++j) {
+          double s = 0.0;
+#pragma unroll
+          for (int k = 0; k < NOC; ++k) s = fma(c_trans[MODE][LC][k][z], wk[i][j][k], s);
+          wsph[i][j] = s;
+        }
+      double wcz[NCA][NCB];
+      weights_to_cart<LA, LB, NOA, NOB>(MODE, wsph, wcz);
+#pragma unroll
+      for (int i = 0; i < NCA; ++i)
+#pragma unroll
+        for (int j = 0; j < NCB; ++j) wsh[slot][(z * NCA + i) * NCB + j] = wcz[i][j];
+    }
+  }
+  __syncthreads();
+  if (work) {
+    {
       const double pair_factor = (pr.x == pr.y) ? 1.0 : 2.0;
       const double* A = xyz + 3 * atomA;
       const double* B = xyz + 3 * atomB;
@@ -362,7 +377,7 @@ __global__ void __launch_bounds__(rp_threads_g3c(LA, LB, LC, SPH),
                   const double dbx = 2.0 * b * ix[ax][bx + 1] - (bx ? bx * ix[ax][bx ? bx - 1 : 0] : 0.0);
                   const double dby = 2.0 * b * iy[ay][by + 1] - (by ? by * iy[ay][by ? by - 1 : 0] : 0.0);
                   const double dbz = 2.0 * b * iz[az][bz + 1] - (bz ? bz * iz[az][bz ? bz - 1 : 0] : 0.0);
-                  const double ww = wr * wc[z][i][j];
+                  const double ww = wr * wsh[slot][(z * NCA + i) * NCB + j];
                   gA[0] = fma(ww, dax * y0 * z0, gA[0]);
                   gA[1] = fma(ww, x0 * day * z0, gA[1]);
                   gA[2] = fma(ww, x0 * y0 * daz, gA[2]);
