@@ -738,7 +738,7 @@ __global__ void __launch_bounds__(kCoulThreads, 1)
   __syncthreads();
   volatile int* ab = &abort_flag;
   const int nitems = p.nmol * p.nao;
-  int issued = 0, consumed = 0;  // producer: tiles issued; producer copy of the consumers' count
+  int issued = 0;  // producer: tiles issued
 
   if (warp == 0) {
     if (lane == 0) {
@@ -825,7 +825,6 @@ __global__ void __launch_bounds__(kCoulThreads, 1)
       }
     }
   }
-  (void)consumed;
 }
 
 // Self-test of the bounded-wait error path: one warp waits on an mbarrier
