@@ -18,7 +18,7 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("nb,n,x,o", [(2, 40, 200, 12), (1, 96, 464, 20), (3, 50, 130, 33),
-                                      (1, 384, 300, 80), (2, 72, 520, 100)])
+                                      (1, 384, 300, 80), (2, 72, 520, 100), (1, 136, 260, 128)])
 def test_half_transform_and_gram(nb, n, x, o):
     ld = (n + 3) // 4 * 4
     o_pad = (o + 15) // 16 * 16
